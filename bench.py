@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark of the tribit_b200 exact triangle counter on B200.
+
+Metric (edges/s = m / count time): the exact count of an RMAT scale-24 graph
+(edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05, seeded, duplicates and
+self-loops removed, ~16.7M vertices, ~250M undirected edges), with synthetic
+data of that shape generated on the host. A step is one launch of the counting
+kernels over the prepared (oriented, bit-packed) graph already resident in
+HBM; preprocessing is timed separately, as the reference reports it. `e2e` is
+the same metric through the public C-ABI call tribit_count_edges on pinned
+host entries: H2D copy, preprocessing, counting and the D2H result inside.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload rmat24|rmat22|rmat20|chung_lu|planted]
+                  [--dispatch auto|plain|learned|bitmap|merge|mma]
+
+Multi-GPU: the counter has no cross-GPU exchange, so N GPUs run N independent
+replicas (seed + rank), one process each under torchrun; value is the sum of
+edges over the max-over-ranks time ("scaling": "weak").
+
+--impl reference times the reference's algorithm on the host cores: the
+reference has no CPU implementation, so this is the CPU merge-intersection
+oracle (a port), timed on a strided sample of 32-row blocks and extrapolated.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edges/s (m / count time) on RMAT-24, learned vs plain dispatch, exact; graphs/s"
+
+WORKLOADS = {
+    "rmat24": {"gen": "rmat", "scale": 24, "edge_factor": 16, "seed": 24},
+    "rmat22": {"gen": "rmat", "scale": 22, "edge_factor": 16, "seed": 22},
+    "rmat20": {"gen": "rmat", "scale": 20, "edge_factor": 16, "seed": 20},
+    "chung_lu": {"gen": "chung_lu", "n": 7115, "n_entries": 115300, "beta": 2.0, "max_degree": 1000.0, "seed": 1},
+    "planted": {"gen": "planted", "communities": 20000, "size": 100, "p_in": 0.3, "inter": 2, "seed": 3},
+}
+
+
+def make_graph(tb, spec, rank):
+    s = dict(spec)
+    seed = s["seed"] + 1000 * rank
+    if s["gen"] == "rmat":
+        return 1 << s["scale"], tb.gen_rmat(s["scale"], s["edge_factor"], 0.57, 0.19, 0.19, seed)
+    if s["gen"] == "chung_lu":
+        return s["n"], tb.gen_chung_lu(s["n"], s["n_entries"], s["beta"], s["max_degree"], seed)
+    if s["gen"] == "planted":
+        return s["communities"] * s["size"], tb.gen_planted(s["communities"], s["size"], s["p_in"], s["inter"], seed)
+    raise ValueError(s["gen"])
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(workload):
+    """Per-launch DRAM bytes of the counting kernels from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == workload:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"tribit_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(entries, n, m, target_s=15.0, steps=1):
+    """Oracle merge-intersection count on a strided sample of 32-row blocks of
+    the degree-ordered CSR, on all host threads; returns per-step results."""
+    import oracle
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    g = oracle.CSR(entries, n, order=1)
+    stride = 1024
+    # Grow the sample until one step costs about target_s of CPU wall time.
+    _, s = g.count_sample(threads, stride, 0)
+    while s < target_s / 8 and stride > 1:
+        stride //= 4 if s < target_s / 64 else 2
+        stride = max(stride, 1)
+        _, s = g.count_sample(threads, stride, 0)
+    out = []
+    for k in range(steps):
+        t, s = g.count_sample(threads, stride, k % stride)
+        full_s = s * stride
+        out.append({"value": m / full_s, "seconds": s, "stride": stride, "offset": k % stride, "sample_triangles": t})
+    g.close()
+    return out, threads
+
+
+def run_reference(args, spec, rank, world):
+    import tribit_b200 as tb
+    if rank != 0:
+        return
+    n, e = make_graph(tb, spec, 0)
+    import oracle
+    m = oracle.count(e[:0], n)[1]  # noqa: F841 (keeps the import warm)
+    edges = int(len(oracle.fold_dedup(e)))
+    steps, threads = cpu_baseline(e, n, edges, steps=args.warmup + args.steps)
+    timed = steps[args.warmup:]
+    value = statistics.mean(x["value"] for x in timed)
+    per_step_s = edges / value
+    line = {
+        "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, **spec, "n": n, "entries": int(len(e)), "edges": edges},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "port",
+                         "sample": f"32-row blocks b % {timed[0]['stride']} == offset (offset per step), "
+                                   f"~{timed[0]['seconds']:.1f} s each, time x stride"},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--dispatch", default="auto")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    spec = WORKLOADS[args.workload]
+
+    if args.impl == "reference":
+        run_reference(args, spec, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import tribit_b200 as tb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    t0 = time.time()
+    n, entries = make_graph(tb, spec, rank)
+    gen_s = time.time() - t0
+
+    dispatch = args.dispatch
+    model_path = os.path.join(ROOT, "tribit_b200", "models", "dispatch_mlp.bin")
+    if dispatch == "auto":
+        dispatch = "learned" if os.path.exists(model_path) else "plain"
+
+    # Inputs resident in HBM for the device-timed value.
+    d_entries = torch.from_numpy(entries.view(np.int64)).to(f"cuda:{local}")
+    stream = torch.cuda.Stream(device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
+
+    def timed_counter(mode):
+        c = tb.Counter(device=local, dispatch=mode)
+        if mode == "learned":
+            c.load_model(model_path)
+        c.set_stream(stream.cuda_stream)
+        prep = c.prepare_device(d_entries.data_ptr(), d_entries.numel(), n)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                flush.fill_(1)
+                c.launch_count()
+            torch.cuda.synchronize()
+            first = c.read_count()
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+            stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+            for k in range(args.steps):
+                flush.fill_(k & 0xff)
+                starts[k].record(stream)
+                c.launch_count()
+                stops[k].record(stream)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+        last = c.read_count()
+        assert last.triangles == first.triangles, "count changed between launches"
+        ms = [a.elapsed_time(b) for a, b in zip(starts, stops)]
+        return c, prep, last, ms
+
+    results = {}
+    modes = [dispatch] + (["plain"] if dispatch == "learned" else [])
+    with ClockSampler(local) as clocks:
+        for mode in modes:
+            c, prep, res, ms = timed_counter(mode)
+            results[mode] = (prep, res, ms)
+            c.close()
+    clk = clocks.summary()
+    prep, res, ms = results[dispatch]
+    total_ms = sum(ms)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    m = res.edges
+    value = world * m / (ms_per_step / 1e3)
+
+    # End to end through the public C-ABI call with pinned host entries.
+    pinned = torch.empty(entries.size, dtype=torch.int64, pin_memory=True)
+    pinned.numpy()[:] = entries.view(np.int64)
+    host = pinned.numpy().view(np.uint64)
+    c = tb.Counter(device=local, dispatch=dispatch)
+    if dispatch == "learned":
+        c.load_model(model_path)
+    c.count_edges(host, n)  # sizes the arena
+    e2e_s = []
+    e2e_res = None
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        e2e_res = c.count_edges(host, n)
+        e2e_s.append(time.perf_counter() - t1)
+    c.close()
+    assert e2e_res.triangles == res.triangles
+    e2e_t = statistics.mean(e2e_s)
+    if dist:
+        t = torch.tensor([e2e_t], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    b_alg = 4 * (n + 1) + 4 * m
+    achieved = b_alg / (ms_per_step / 1e3) / 1e9
+    traffic = profiled_traffic(args.workload)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        steps, threads = cpu_baseline(entries, n, m, steps=1)
+        x = steps[0]
+        cpu = {"value": x["value"], "unit": "edges/s", "cores": threads, "kind": "port",
+               "sample": f"oracle merge count of 32-row blocks b % {x['stride']} == 0 of the degree-ordered CSR "
+                         f"({x['seconds']:.1f} s), time x {x['stride']}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": args.workload, **spec, "n": n, "entries": int(entries.size), "edges": m,
+                       "triangles": res.triangles, "dispatch": dispatch, "parallelism": f"replicas{world}",
+                       "l2": "256 MiB buffer written between timed steps; inputs > L2",
+                       "preprocess_ms": prep.preprocess_ms, "gen_s": round(gen_s, 2),
+                       "row_blocks_by_variant": dict(zip(tb.VARIANTS, res.row_blocks_by_variant)),
+                       "per_mode_edges_per_s": {k: world * v[1].edges / (sum(v[2]) / len(v[2]) / 1e3)
+                                                for k, v in results.items()}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes": b_alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * m / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
+                    "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3},
+            "clocks": clk,
+            "gpu_launches": args.steps * res.count_kernels,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/* tribit_b200 -- exact triangle counting on one NVIDIA B200 (sm_100a).
+ *
+ * C-ABI boundary of the counter. Plain pointers and sizes only; every entry
+ * point returns a tribit_status and never exits the process.
+ *
+ * Reference interfaces replaced (paths within sixt99/TriBIT):
+ *   count_triangles(zipped, nnz, cfg, print)  src/single_gpu/tribit.cu:656
+ *     -> tribit_count_edges / tribit_count_edges_device
+ *   read_mtx(path, zipped)                     src/single_gpu/tribit.cu:228
+ *     -> tribit_read_mtx, tribit_count_mtx
+ *   allocate_memory() + cudaMalloc_log pool    src/single_gpu/tribit.cu:825, :48
+ *     -> tribit_create (per-device context owning a reusable device arena)
+ *   init_gpu_kernel5(gpu_id)                   src/multi_gpu/cuda/main5_multi.cu:578
+ *     -> tribit_create (options.device)
+ *   count_partial_triangles_diagonal(...)      src/multi_gpu/cuda/main5_multi.cu:589
+ *     (the reference's FFI precedent, declared at src/multi_gpu/src/main.rs:15-36)
+ *     -> tribit_count_edges (host zipped entries in, uint64 count out)
+ *   main / program_options                     src/single_gpu/tribit.cu:282, :840
+ *     -> the `tribit` CLI, a thin caller of this header
+ *
+ * Entry words use the reference's zipped layout (a << 32) | b with 0-based
+ * vertex ids (tribit.cu:258-266). The counter folds each entry to
+ * (min, max), drops self-loops (a == b) and deduplicates, so both the folded
+ * words read_mtx produces and raw, unfolded edge lists are accepted.
+ *
+ * Threading: a context belongs to one device and may be used by one host
+ * thread at a time. Distinct contexts are independent.
+ */
+#ifndef TRIBIT_H
+#define TRIBIT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tribit_status {
+  TRIBIT_OK = 0,
+  TRIBIT_ERR_INVALID_ARGUMENT = 1,
+  TRIBIT_ERR_IO = 2,          /* cannot open / read / write a file        (ref: tribit.cu:230 throws) */
+  TRIBIT_ERR_FORMAT = 3,      /* malformed Matrix Market size line         */
+  TRIBIT_ERR_NOT_SQUARE = 4,  /* rows != cols                              (ref: tribit.cu:241-245 throws) */
+  TRIBIT_ERR_ID_RANGE = 5,    /* an entry names a vertex >= num_nodes      (ref: unchecked) */
+  TRIBIT_ERR_TOO_LARGE = 6,   /* beyond the 32-bit id / edge-count limits  (ref: tribit.cu:773 throws) */
+  TRIBIT_ERR_CUDA = 7,        /* CUDA runtime error; see tribit_last_error */
+  TRIBIT_ERR_OUT_OF_MEMORY = 8, /* device or host allocation failed      (ref: tribit.cu:62-65 exit(1)) */
+  TRIBIT_ERR_NO_DEVICE = 9,   /* no usable CUDA device                     */
+  TRIBIT_ERR_TIMEOUT = 10,    /* a bounded device-side wait gave up        */
+  TRIBIT_ERR_NO_MODEL = 11,   /* learned dispatch requested without a model */
+  TRIBIT_ERR_INTERNAL = 12
+} tribit_status;
+
+/* Vertex orientation: every triangle is counted once, at its lowest vertex. */
+enum {
+  TRIBIT_ORDER_DEGREE = 0, /* rank by (degree, id), orient low -> high rank (default) */
+  TRIBIT_ORDER_ID = 1      /* orient u -> v iff u < v, as the reference does (tribit.cu:261-267) */
+};
+
+/* How each 32-row block of the oriented graph picks its counting variant. */
+enum {
+  TRIBIT_DISPATCH_PLAIN = 0,   /* fixed thresholds on row-block features */
+  TRIBIT_DISPATCH_LEARNED = 1, /* MLP over row-block features (tribit_model_*) */
+  TRIBIT_DISPATCH_MERGE = 2,   /* force sorted-list merge everywhere */
+  TRIBIT_DISPATCH_BITMAP = 3,  /* force LOP3 + popc on bit-packed rows everywhere */
+  TRIBIT_DISPATCH_MMA = 4      /* force b1 AND+POPC tensor-core tiles everywhere */
+};
+
+/* Counting variants, in the order used by per-variant arrays below. */
+enum { TRIBIT_VARIANT_MMA = 0, TRIBIT_VARIANT_BITMAP = 1, TRIBIT_VARIANT_MERGE = 2, TRIBIT_NUM_VARIANTS = 3 };
+
+typedef struct tribit_options {
+  int device;            /* CUDA device ordinal */
+  int order;             /* TRIBIT_ORDER_* */
+  int dispatch;          /* TRIBIT_DISPATCH_* */
+  int ctas_per_sm;       /* counting-kernel CTAs per SM; 0 = tuned default */
+  uint32_t reserved[8];  /* must be zero */
+} tribit_options;
+
+typedef struct tribit_result {
+  uint64_t triangles;         /* exact count */
+  uint64_t num_nodes;         /* n as given */
+  uint64_t entries;           /* input entries */
+  uint64_t edges;             /* undirected edges after fold, self-loop removal, dedup */
+  uint64_t blocks_of_threads; /* CTAs of the counting launch ("Blocks of threads") */
+  uint64_t row_blocks;        /* non-empty 32-row blocks of the oriented graph */
+  uint64_t row_blocks_by_variant[TRIBIT_NUM_VARIANTS];
+  float h2d_ms;               /* host -> device copy of the entries (host-input calls) */
+  float preprocess_ms;        /* fold, dedup, orient, CSR and bit-block build */
+  float kernel_ms;            /* counting kernel(s) */
+  float total_ms;             /* whole call, device time */
+  uint32_t count_kernels;     /* kernels one counting launch issues */
+  uint32_t reserved;
+} tribit_result;
+
+typedef struct tribit_context tribit_context;
+
+/* ---- context --------------------------------------------------------- */
+void tribit_default_options(tribit_options* opts);
+tribit_status tribit_create(const tribit_options* opts, tribit_context** ctx);
+void tribit_destroy(tribit_context* ctx);
+/* Run all later work of this context on `cuda_stream` (a cudaStream_t; NULL
+ * restores the context's own stream). */
+tribit_status tribit_set_stream(tribit_context* ctx, void* cuda_stream);
+const char* tribit_status_string(tribit_status st);
+const char* tribit_last_error(const tribit_context* ctx);
+const char* tribit_version(void);
+
+/* ---- single graph ------------------------------------------------------ */
+/* Host entries -> exact count (H2D copy, preprocessing, counting, D2H). */
+tribit_status tribit_count_edges(tribit_context* ctx, const uint64_t* entries, uint64_t n_entries, uint64_t num_nodes,
+                                 tribit_result* out);
+/* Same with the entries already in device memory. */
+tribit_status tribit_count_edges_device(tribit_context* ctx, const uint64_t* d_entries, uint64_t n_entries,
+                                        uint64_t num_nodes, tribit_result* out);
+/* Two-phase form: build the oriented, bit-packed graph once, then launch the
+ * counting kernel(s) any number of times. tribit_launch_count only enqueues
+ * work on the context's stream; tribit_read_count waits and returns it. */
+tribit_status tribit_prepare_device(tribit_context* ctx, const uint64_t* d_entries, uint64_t n_entries,
+                                    uint64_t num_nodes, tribit_result* out);
+tribit_status tribit_launch_count(tribit_context* ctx);
+tribit_status tribit_read_count(tribit_context* ctx, tribit_result* out);
+
+/* ---- Matrix Market ------------------------------------------------------ */
+/* Reads a coordinate .mtx with the reference's semantics (tribit.cu:228-269):
+ * banner line, '%' lines skipped, "rows cols nnz", rows must equal cols,
+ * 1-based "r c [values...]" entries, values ignored, self-loops dropped, each
+ * entry folded to (min << 32) | max. *entries is allocated with malloc and
+ * released with tribit_free_host. */
+tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, uint64_t** entries, uint64_t* n_entries);
+void tribit_free_host(void* p);
+tribit_status tribit_count_mtx(tribit_context* ctx, const char* path, tribit_result* out);
+
+/* ---- batches ----------------------------------------------------------- */
+/* num_graphs independent graphs in one persistent counting launch. Graph g's
+ * entries are entries[entry_offsets[g] .. entry_offsets[g + 1]) with vertex
+ * ids in [0, num_nodes[g]). triangles_out[g] receives graph g's exact count. */
+tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, const uint64_t* entry_offsets,
+                                 const uint32_t* num_nodes, uint32_t num_graphs, uint64_t* triangles_out,
+                                 tribit_result* out);
+
+/* ---- learned dispatcher ------------------------------------------------- */
+/* Loads MLP weights (16 -> 64 -> 64 -> 3) written by tribit_model_save. */
+tribit_status tribit_model_load(tribit_context* ctx, const char* path);
+
+/* ---- synthetic graphs (host, seeded, thread-count independent) ---------- */
+tribit_status tribit_gen_rmat(int scale, uint64_t edge_factor, double a, double b, double c, uint64_t seed,
+                              uint64_t* out);
+tribit_status tribit_gen_er(uint32_t n, uint64_t n_entries, uint64_t seed, uint64_t* out);
+tribit_status tribit_gen_chung_lu(uint32_t n, uint64_t n_entries, double beta, double max_degree, uint64_t seed,
+                                  uint64_t* out);
+tribit_status tribit_gen_planted(uint32_t communities, uint32_t size, double p_in, uint32_t inter_per_vertex,
+                                 uint64_t seed, uint64_t* out, uint64_t* n_entries);
+tribit_status tribit_write_mtx(const char* path, uint64_t num_nodes, const uint64_t* entries, uint64_t n_entries);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

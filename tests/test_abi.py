@@ -1,0 +1,78 @@
+"""The C-ABI library: loads without a GPU, exports every declared symbol,
+maps statuses, and its host-side generators are deterministic."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import tribit_b200 as tb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names += re.findall(r"\b(tribit_[a-z0-9_]+)\s*\(", txt)
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 20
+    so = ctypes.CDLL(tb.LIB_PATH)
+    missing = [n for n in names if not hasattr(so, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    for s in range(0, 13):
+        assert tb.lib.tribit_status_string(s)
+    assert tb.lib.tribit_status_string(999) == b"unknown status"
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) is None and os.path.exists("/dev/nvidia0"),
+                    reason="a GPU is present")
+def test_no_device_status():
+    with pytest.raises(tb.TribitError) as ex:
+        tb.Counter()
+    assert ex.value.status == 9
+
+
+def test_invalid_arguments():
+    assert tb.lib.tribit_count_edges(None, None, 0, 0, None) == 1
+    assert tb.lib.tribit_launch_count(None) == 1
+    assert tb.lib.tribit_set_stream(None, None) == 1
+
+
+def test_generators_deterministic():
+    a = tb.gen_rmat(12, 16, seed=5)
+    b = tb.gen_rmat(12, 16, seed=5)
+    c = tb.gen_rmat(12, 16, seed=6)
+    np.testing.assert_array_equal(a, b)
+    assert not np.array_equal(a, c)
+    assert a.size == 16 << 12
+    assert int((a >> np.uint64(32)).max()) < 4096 and int((a & np.uint64(0xFFFFFFFF)).max()) < 4096
+    # large enough to run on several host threads: still identical
+    x = tb.gen_rmat(16, 16, seed=5)
+    np.testing.assert_array_equal(x, tb.gen_rmat(16, 16, seed=5))
+    e = tb.gen_er(1000, 100000, seed=1)
+    assert int((e >> np.uint64(32)).max()) < 1000
+    cl = tb.gen_chung_lu(5000, 50000, 2.1, 300.0, seed=2)
+    np.testing.assert_array_equal(cl, tb.gen_chung_lu(5000, 50000, 2.1, 300.0, seed=2))
+    p = tb.gen_planted(50, 20, 0.5, 2, seed=3)
+    assert int((p >> np.uint64(32)).max()) < 1000
+    np.testing.assert_array_equal(p, tb.gen_planted(50, 20, 0.5, 2, seed=3))
+
+
+def test_rmat_skew():
+    e = tb.gen_rmat(14, 16, seed=1)
+    r = (e >> np.uint64(32)).astype(np.int64)
+    # quadrant a+b = 0.76 per level: vertex 0 is by far the heaviest row
+    counts = np.bincount(r, minlength=1 << 14)
+    assert counts.argmax() == 0

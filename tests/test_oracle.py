@@ -1,0 +1,87 @@
+"""The CPU oracle against closed-form known answers and the golden fixtures."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import tribit_b200 as tb
+from tests.graphs import clique, comb, numpy_count, star, wheel, zip_pairs
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_counts.json")))
+
+
+@pytest.mark.parametrize("n", [3, 4, 5, 10, 33, 64, 100])
+def test_clique(n):
+    e = clique(n)
+    for order in (0, 1):
+        assert oracle.count(e, n, order=order) == (comb(n), n * (n - 1) // 2)
+    assert oracle.count_tribit(e, n)[0] == comb(n)
+
+
+@pytest.mark.parametrize("n", [5, 6, 40, 100])
+def test_wheel(n):
+    assert oracle.count(wheel(n), n)[0] == n - 1
+    assert oracle.count_tribit(wheel(n), n)[0] == n - 1
+
+
+def test_star_empty_single():
+    assert oracle.count(star(50), 50) == (0, 49)
+    assert oracle.count(np.zeros(0, dtype=np.uint64), 10) == (0, 0)
+    assert oracle.count(zip_pairs([(0, 1), (1, 2), (0, 2)]), 3) == (1, 3)
+    assert oracle.count_tribit(np.zeros(0, dtype=np.uint64), 10) == (0, 0)
+
+
+def test_duplicates_selfloops_unfolded():
+    base = zip_pairs([(0, 1), (1, 2), (2, 0), (2, 3), (3, 0)])
+    noisy = np.concatenate([base, zip_pairs([(1, 0), (2, 1), (0, 2), (3, 3), (1, 1), (0, 1), (3, 2)])])
+    assert oracle.count(noisy, 4) == oracle.count(base, 4) == (2, 5)
+
+
+def test_disjoint_cliques():
+    e = np.concatenate([clique(k, base=sum(range(3, k))) for k in range(3, 12)])
+    n = sum(range(3, 12))
+    assert oracle.count(e, n)[0] == sum(comb(k) for k in range(3, 12))
+
+
+def test_random_against_dense_numpy():
+    rng = np.random.default_rng(0)
+    for trial in range(20):
+        n = int(rng.integers(2, 120))
+        m = int(rng.integers(0, 2000))
+        a = rng.integers(0, n, size=m, dtype=np.uint64)
+        b = rng.integers(0, n, size=m, dtype=np.uint64)
+        e = (a << np.uint64(32)) | b
+        want = numpy_count(e, n)
+        assert oracle.count(e, n, order=0)[0] == want
+        assert oracle.count(e, n, order=1)[0] == want
+        assert oracle.count_tribit(e, n)[0] == want
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN if c["name"] != "wiki-Vote" and c["entries"] <= 400000],
+                         ids=lambda c: c["name"])
+def test_golden_generated(case):
+    from tests.golden.make_golden import checksum, generate
+    n, e = generate(case["params"])
+    assert checksum(e) == case["entries_sha256_16"], "generator output drifted"
+    t, m = oracle.count(e, n)
+    assert (t, m) == (case["triangles"], case["edges"])
+    assert oracle.count_tribit(e, n) == (case["triangles"], case["reference_blocks_of_threads"])
+
+
+@pytest.mark.skipif(not os.path.exists("/root/reference/wiki-Vote.mtx"), reason="reference tree not mounted")
+def test_wiki_vote_reference_fixture():
+    rec = [c for c in GOLDEN if c["name"] == "wiki-Vote"][0]
+    st, n, e = oracle.read_mtx("/root/reference/wiki-Vote.mtx")
+    assert st == 0 and n == rec["num_nodes"] == 8297 and len(e) == rec["entries"]
+    assert oracle.count(e, n) == (608389, 100762)
+    assert oracle.count_tribit(e, n) == (608389, 28449)
+
+
+def test_row_counts_sum():
+    e = tb.gen_rmat(11, 8, seed=3)
+    g = oracle.CSR(e, 1 << 11)
+    rows = g.row_counts()
+    t, _ = g.count(threads=4)
+    assert int(rows.sum()) == t == oracle.count(e, 1 << 11)[0]

@@ -1,0 +1,255 @@
+"""tribit_b200 -- exact triangle counting on one NVIDIA B200 (sm_100a).
+
+Python binding of the C-ABI in ``include/tribit.h`` (ctypes over the in-tree
+``libtribit.so``). It mirrors the reference single-GPU counter of
+sixt99/TriBIT: ``read_mtx`` follows ``read_mtx`` (src/single_gpu/tribit.cu:228)
+and ``Counter.count_edges`` follows ``count_triangles``
+(src/single_gpu/tribit.cu:656) -- same zipped (a << 32) | b input words, same
+exact uint64 count -- with status codes raised as ``TribitError`` instead of
+process exits.
+
+There is no CPU fallback: importing this package without the built library
+raises ImportError, and every count runs the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = [
+    "TribitError", "Counter", "Result", "read_mtx", "write_mtx", "gen_rmat", "gen_er",
+    "gen_chung_lu", "gen_planted", "lib", "LIB_PATH", "ORDERS", "DISPATCH", "VARIANTS",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtribit.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing; build it with `make -C tribit_b200` "
+        "(or __graft_entry__.build()). tribit_b200 has no CPU fallback.")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+ORDERS = {"degree": 0, "id": 1}
+DISPATCH = {"plain": 0, "learned": 1, "merge": 2, "bitmap": 3, "mma": 4}
+VARIANTS = ("mma", "bitmap", "merge")
+
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+_p = ctypes.c_void_p
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("order", ctypes.c_int), ("dispatch", ctypes.c_int),
+                ("ctas_per_sm", ctypes.c_int), ("reserved", _u32 * 8)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("triangles", _u64), ("num_nodes", _u64), ("entries", _u64), ("edges", _u64),
+                ("blocks_of_threads", _u64), ("row_blocks", _u64), ("row_blocks_by_variant", _u64 * 3),
+                ("h2d_ms", ctypes.c_float), ("preprocess_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
+                ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("reserved", _u32)]
+
+
+def _decl(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_decl("tribit_default_options", None, ctypes.POINTER(_Options))
+_decl("tribit_create", ctypes.c_int, ctypes.POINTER(_Options), ctypes.POINTER(_p))
+_decl("tribit_destroy", None, _p)
+_decl("tribit_set_stream", ctypes.c_int, _p, _p)
+_decl("tribit_status_string", ctypes.c_char_p, ctypes.c_int)
+_decl("tribit_last_error", ctypes.c_char_p, _p)
+_decl("tribit_version", ctypes.c_char_p)
+_decl("tribit_count_edges", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
+_decl("tribit_count_edges_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
+_decl("tribit_prepare_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
+_decl("tribit_launch_count", ctypes.c_int, _p)
+_decl("tribit_read_count", ctypes.c_int, _p, ctypes.POINTER(_Result))
+_decl("tribit_read_mtx", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_p), ctypes.POINTER(_u64))
+_decl("tribit_free_host", None, _p)
+_decl("tribit_count_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
+_decl("tribit_count_batch", ctypes.c_int, _p, _p, _p, _p, _u32, _p, ctypes.POINTER(_Result))
+_decl("tribit_model_load", ctypes.c_int, _p, ctypes.c_char_p)
+_decl("tribit_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, _p)
+_decl("tribit_gen_er", ctypes.c_int, _u32, _u64, _u64, _p)
+_decl("tribit_gen_chung_lu", ctypes.c_int, _u32, _u64, ctypes.c_double, ctypes.c_double, _u64, _p)
+_decl("tribit_gen_planted", ctypes.c_int, _u32, _u32, ctypes.c_double, _u32, _u64, _p, ctypes.POINTER(_u64))
+_decl("tribit_write_mtx", ctypes.c_int, ctypes.c_char_p, _u64, _p, _u64)
+
+
+class TribitError(RuntimeError):
+    """A non-zero tribit_status from the C-ABI."""
+
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        msg = lib.tribit_status_string(status).decode()
+        super().__init__(f"{msg} (status {status})" + (f": {detail}" if detail else ""))
+
+
+def _check(st: int, ctx=None):
+    if st != 0:
+        detail = lib.tribit_last_error(ctx).decode() if ctx else ""
+        raise TribitError(st, detail)
+
+
+@dataclass
+class Result:
+    triangles: int
+    num_nodes: int
+    entries: int
+    edges: int
+    blocks_of_threads: int
+    row_blocks: int
+    row_blocks_by_variant: tuple
+    h2d_ms: float
+    preprocess_ms: float
+    kernel_ms: float
+    total_ms: float
+    count_kernels: int
+
+    @classmethod
+    def _from(cls, r: _Result) -> "Result":
+        return cls(r.triangles, r.num_nodes, r.entries, r.edges, r.blocks_of_threads, r.row_blocks,
+                   tuple(r.row_blocks_by_variant), r.h2d_ms, r.preprocess_ms, r.kernel_ms, r.total_ms,
+                   r.count_kernels)
+
+
+def _entries(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a
+
+
+class Counter:
+    """A tribit context on one CUDA device (tribit_create / tribit_destroy)."""
+
+    def __init__(self, device: int = 0, order: str = "degree", dispatch: str = "plain", ctas_per_sm: int = 0):
+        o = _Options()
+        lib.tribit_default_options(ctypes.byref(o))
+        o.device = device
+        o.order = ORDERS[order]
+        o.dispatch = DISPATCH[dispatch]
+        o.ctas_per_sm = ctas_per_sm
+        h = _p()
+        _check(lib.tribit_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.tribit_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib.tribit_set_stream(self._h, stream_ptr or None), self._h)
+
+    def load_model(self, path: str):
+        _check(lib.tribit_model_load(self._h, path.encode()), self._h)
+
+    def count_edges(self, entries, num_nodes: int) -> Result:
+        e = _entries(entries)
+        r = _Result()
+        _check(lib.tribit_count_edges(self._h, e.ctypes.data, e.size, int(num_nodes), ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def count_edges_device(self, ptr: int, n_entries: int, num_nodes: int) -> Result:
+        r = _Result()
+        _check(lib.tribit_count_edges_device(self._h, ptr, n_entries, int(num_nodes), ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def prepare_device(self, ptr: int, n_entries: int, num_nodes: int) -> Result:
+        r = _Result()
+        _check(lib.tribit_prepare_device(self._h, ptr, n_entries, int(num_nodes), ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def launch_count(self):
+        _check(lib.tribit_launch_count(self._h), self._h)
+
+    def read_count(self) -> Result:
+        r = _Result()
+        _check(lib.tribit_read_count(self._h, ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def count_mtx(self, path: str) -> Result:
+        r = _Result()
+        _check(lib.tribit_count_mtx(self._h, path.encode(), ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def count_batch(self, entries, offsets, num_nodes):
+        """Counts len(num_nodes) graphs in one launch; returns (counts, Result)."""
+        e = _entries(entries)
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        nn = np.ascontiguousarray(num_nodes, dtype=np.uint32)
+        g = nn.size
+        if off.size != g + 1:
+            raise ValueError("offsets must have len(num_nodes) + 1 entries")
+        out = np.zeros(g, dtype=np.uint64)
+        r = _Result()
+        _check(lib.tribit_count_batch(self._h, e.ctypes.data if e.size else None, off.ctypes.data, nn.ctypes.data, g,
+                                      out.ctypes.data, ctypes.byref(r)), self._h)
+        return out, Result._from(r)
+
+
+def read_mtx(path: str):
+    """Reads a Matrix Market file with the reference's semantics -> (num_nodes, entries)."""
+    n = _u64()
+    ptr = _p()
+    cnt = _u64()
+    _check(lib.tribit_read_mtx(str(path).encode(), ctypes.byref(n), ctypes.byref(ptr), ctypes.byref(cnt)))
+    try:
+        buf = (ctypes.c_uint64 * max(cnt.value, 1)).from_address(ptr.value)
+        arr = np.frombuffer(buf, dtype=np.uint64, count=cnt.value).copy()
+    finally:
+        lib.tribit_free_host(ptr)
+    return n.value, arr
+
+
+def write_mtx(path: str, num_nodes: int, entries):
+    e = _entries(entries)
+    _check(lib.tribit_write_mtx(str(path).encode(), num_nodes, e.ctypes.data, e.size))
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1) -> np.ndarray:
+    out = np.empty(edge_factor << scale, dtype=np.uint64)
+    _check(lib.tribit_gen_rmat(scale, edge_factor, a, b, c, seed, out.ctypes.data))
+    return out
+
+
+def gen_er(n: int, n_entries: int, seed: int = 1) -> np.ndarray:
+    out = np.empty(n_entries, dtype=np.uint64)
+    _check(lib.tribit_gen_er(n, n_entries, seed, out.ctypes.data))
+    return out
+
+
+def gen_chung_lu(n: int, n_entries: int, beta: float, max_degree: float, seed: int = 1) -> np.ndarray:
+    out = np.empty(n_entries, dtype=np.uint64)
+    _check(lib.tribit_gen_chung_lu(n, n_entries, beta, max_degree, seed, out.ctypes.data))
+    return out
+
+
+def gen_planted(communities: int, size: int, p_in: float, inter_per_vertex: int, seed: int = 1) -> np.ndarray:
+    cnt = _u64(0)
+    _check(lib.tribit_gen_planted(communities, size, p_in, inter_per_vertex, seed, None, ctypes.byref(cnt)))
+    out = np.empty(cnt.value, dtype=np.uint64)
+    _check(lib.tribit_gen_planted(communities, size, p_in, inter_per_vertex, seed, out.ctypes.data, ctypes.byref(cnt)))
+    return out

@@ -1,0 +1,374 @@
+// C-ABI entry points (include/tribit.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "arena.h"
+#include "common.cuh"
+#include "count.cuh"
+#include "prep.cuh"
+#include "tribit.h"
+
+struct tribit_context {
+  tribit_options opts{};
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t st = nullptr;
+  tb::Arena arena;
+  tb::Prepared prep{};
+  tb::Schedule sched{};
+  unsigned long long* per_graph = nullptr;
+  bool prepared = false;
+  tb::LaunchInfo launch{};
+  cudaEvent_t ev[6] = {};
+  tb::DeviceStats* h_stats = nullptr;  // pinned
+  std::string err;
+};
+
+namespace {
+
+using tb::CudaError;
+using tb::StatusError;
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+template <typename F>
+tribit_status guarded(tribit_context* ctx, F&& body) {
+  try {
+    body();
+    return TRIBIT_OK;
+  } catch (const StatusError& e) {
+    if (ctx) ctx->err = e.what();
+    return e.status;
+  } catch (const CudaError& e) {
+    if (ctx) ctx->err = e.what();
+    return e.code == cudaErrorMemoryAllocation ? TRIBIT_ERR_OUT_OF_MEMORY : TRIBIT_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    if (ctx) ctx->err = "host allocation failed";
+    return TRIBIT_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->err = e.what();
+    return TRIBIT_ERR_INTERNAL;
+  }
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  TB_CUDA(cudaEventElapsedTime(&ms, a, b));
+  return ms;
+}
+
+// Device buffers of one call, laid out identically in the measuring pass and
+// the real pass.
+struct CallLayout {
+  uint64_t* staged = nullptr;     // host-input calls: device copy of the entries
+  uint64_t* eoff = nullptr;       // batch: entry offsets
+  uint64_t* voff = nullptr;       // batch: vertex offsets
+  unsigned long long* per_graph = nullptr;
+};
+
+void layout(tribit_context* c, bool measure, const tb::PrepInput& in, bool stage, uint32_t G, CallLayout* L) {
+  tb::Arena& ar = c->arena;
+  ar.begin(measure);
+  L->staged = stage ? ar.take<uint64_t>(in.E ? in.E : 1) : nullptr;
+  if (G) {
+    L->eoff = ar.take<uint64_t>(G + 1);
+    L->voff = ar.take<uint64_t>(G + 1);
+    L->per_graph = ar.take<unsigned long long>(G);
+  }
+  tb::PrepInput pin = in;
+  if (stage) pin.entries = L->staged;
+  if (G) {
+    pin.eoff = L->eoff;
+    pin.voff = L->voff;
+  }
+  if (!measure) return;
+  // Measuring: walk the same takes prepare_graph / take_schedule will do.
+  tb::Prepared tmp;
+  tb::prepare_graph(ar, pin, c->st, &tmp);
+  (void)tb::take_schedule(ar, in.n);
+}
+
+// Runs preprocessing + schedule (+ counting when count == true) for one input.
+void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries, const uint64_t* host_eoff,
+              const uint64_t* host_voff, uint32_t G, bool count, tribit_result* res) {
+  DeviceGuard dg(c->device);
+  const bool stage = host_entries != nullptr;
+  CallLayout L;
+  layout(c, true, in, stage, G, &L);
+  c->arena.reserve(c->arena.used());
+  layout(c, false, in, stage, G, &L);
+  cudaStream_t st = c->st;
+  TB_CUDA(cudaEventRecord(c->ev[0], st));
+  if (stage && in.E) TB_CUDA(cudaMemcpyAsync(L.staged, host_entries, in.E * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  if (G) {
+    TB_CUDA(cudaMemcpyAsync(L.eoff, host_eoff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    TB_CUDA(cudaMemcpyAsync(L.voff, host_voff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    TB_CUDA(cudaMemsetAsync(L.per_graph, 0, G * sizeof(unsigned long long), st));
+  }
+  TB_CUDA(cudaEventRecord(c->ev[1], st));
+  tb::PrepInput pin = in;
+  if (stage) pin.entries = L.staged;
+  if (G) {
+    pin.eoff = L.eoff;
+    pin.voff = L.voff;
+  }
+  tb::prepare_graph(c->arena, pin, st, &c->prep);
+  c->sched = tb::take_schedule(c->arena, in.n);
+  tb::build_schedule(c->prep.view, c->sched, c->opts.dispatch, nullptr, st);
+  c->per_graph = L.per_graph;
+  c->prepared = true;
+  TB_CUDA(cudaEventRecord(c->ev[2], st));
+  if (count) {
+    tb::CountConfig cfg;
+    cfg.num_sms = c->num_sms;
+    cfg.ctas_per_sm = c->opts.ctas_per_sm;
+    c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, L.per_graph, cfg, st);
+  }
+  TB_CUDA(cudaEventRecord(c->ev[3], st));
+  TB_CUDA(cudaMemcpyAsync(c->h_stats, c->prep.stats, sizeof(tb::DeviceStats), cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaEventRecord(c->ev[4], st));
+  TB_CUDA(cudaEventSynchronize(c->ev[4]));
+  TB_CUDA(cudaGetLastError());
+  const tb::DeviceStats& hs = *c->h_stats;
+  if (hs.err & tb::kErrIdRange) throw StatusError(TRIBIT_ERR_ID_RANGE, "an entry names a vertex id >= num_nodes");
+  if (hs.err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
+  if (res) {
+    std::memset(res, 0, sizeof *res);
+    res->triangles = count ? hs.triangles : 0;
+    res->num_nodes = in.n;
+    res->entries = in.E;
+    res->edges = hs.edges;
+    res->blocks_of_threads = count ? c->launch.ctas : 0;
+    res->count_kernels = c->launch.kernels;
+    res->h2d_ms = elapsed(c->ev[0], c->ev[1]);
+    res->preprocess_ms = elapsed(c->ev[1], c->ev[2]);
+    res->kernel_ms = count ? elapsed(c->ev[2], c->ev[3]) : 0.f;
+    res->total_ms = elapsed(c->ev[0], c->ev[4]);
+  }
+}
+
+void fill_schedule_stats(tribit_context* c, tribit_result* res) {
+  uint32_t lens[TRIBIT_NUM_VARIANTS];
+  TB_CUDA(cudaMemcpyAsync(lens, c->sched.list_len, sizeof lens, cudaMemcpyDeviceToHost, c->st));
+  TB_CUDA(cudaStreamSynchronize(c->st));
+  res->row_blocks = 0;
+  for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) {
+    res->row_blocks_by_variant[v] = lens[v];
+    res->row_blocks += lens[v];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void tribit_default_options(tribit_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->order = TRIBIT_ORDER_DEGREE;
+  o->dispatch = TRIBIT_DISPATCH_PLAIN;
+}
+
+const char* tribit_version(void) { return "tribit_b200 0.1.0 (sm_100a)"; }
+
+const char* tribit_status_string(tribit_status s) {
+  switch (s) {
+    case TRIBIT_OK: return "ok";
+    case TRIBIT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case TRIBIT_ERR_IO: return "cannot open or read file";
+    case TRIBIT_ERR_FORMAT: return "malformed Matrix Market file";
+    case TRIBIT_ERR_NOT_SQUARE: return "matrix is not square";
+    case TRIBIT_ERR_ID_RANGE: return "vertex id out of range";
+    case TRIBIT_ERR_TOO_LARGE: return "graph exceeds 32-bit limits";
+    case TRIBIT_ERR_CUDA: return "CUDA error";
+    case TRIBIT_ERR_OUT_OF_MEMORY: return "out of memory";
+    case TRIBIT_ERR_NO_DEVICE: return "no CUDA device";
+    case TRIBIT_ERR_TIMEOUT: return "device wait timed out";
+    case TRIBIT_ERR_NO_MODEL: return "no dispatcher model loaded";
+    case TRIBIT_ERR_INTERNAL: return "internal error";
+  }
+  return "unknown status";
+}
+
+const char* tribit_last_error(const tribit_context* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+tribit_status tribit_create(const tribit_options* opts, tribit_context** out) {
+  if (!out) return TRIBIT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  tribit_options o;
+  tribit_default_options(&o);
+  if (opts) o = *opts;
+  if (o.order != TRIBIT_ORDER_DEGREE && o.order != TRIBIT_ORDER_ID) return TRIBIT_ERR_INVALID_ARGUMENT;
+  if (o.dispatch < TRIBIT_DISPATCH_PLAIN || o.dispatch > TRIBIT_DISPATCH_MMA) return TRIBIT_ERR_INVALID_ARGUMENT;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    (void)cudaGetLastError();
+    return TRIBIT_ERR_NO_DEVICE;
+  }
+  if (o.device < 0 || o.device >= count) return TRIBIT_ERR_INVALID_ARGUMENT;
+  tribit_context* c = new (std::nothrow) tribit_context();
+  if (!c) return TRIBIT_ERR_OUT_OF_MEMORY;
+  c->opts = o;
+  c->device = o.device;
+  tribit_status st = guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    TB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+    TB_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+    c->st = c->own;
+    for (auto& e : c->ev) TB_CUDA(cudaEventCreate(&e));
+    TB_CUDA(cudaMallocHost(&c->h_stats, sizeof(tb::DeviceStats)));
+  });
+  if (st != TRIBIT_OK) {
+    tribit_destroy(c);
+    return st;
+  }
+  *out = c;
+  return TRIBIT_OK;
+}
+
+void tribit_destroy(tribit_context* c) {
+  if (!c) return;
+  {
+    DeviceGuard dg(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    c->arena.release();
+    for (auto& e : c->ev)
+      if (e) cudaEventDestroy(e);
+    if (c->h_stats) cudaFreeHost(c->h_stats);
+    if (c->own) cudaStreamDestroy(c->own);
+  }
+  delete c;
+}
+
+tribit_status tribit_set_stream(tribit_context* c, void* stream) {
+  if (!c) return TRIBIT_ERR_INVALID_ARGUMENT;
+  c->st = stream ? (cudaStream_t)stream : c->own;
+  return TRIBIT_OK;
+}
+
+tribit_status tribit_count_edges(tribit_context* c, const uint64_t* entries, uint64_t n_entries, uint64_t num_nodes,
+                                 tribit_result* out) {
+  if (!c || (!entries && n_entries)) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    tb::PrepInput in;
+    in.E = n_entries;
+    in.n = num_nodes;
+    in.order = c->opts.order;
+    static const uint64_t dummy = 0;
+    run_call(c, in, entries ? entries : &dummy, nullptr, nullptr, 0, true, out);
+    if (out) fill_schedule_stats(c, out);
+  });
+}
+
+tribit_status tribit_count_edges_device(tribit_context* c, const uint64_t* d_entries, uint64_t n_entries,
+                                        uint64_t num_nodes, tribit_result* out) {
+  if (!c || (!d_entries && n_entries)) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    tb::PrepInput in;
+    in.entries = d_entries;
+    in.E = n_entries;
+    in.n = num_nodes;
+    in.order = c->opts.order;
+    run_call(c, in, nullptr, nullptr, nullptr, 0, true, out);
+    if (out) fill_schedule_stats(c, out);
+  });
+}
+
+tribit_status tribit_prepare_device(tribit_context* c, const uint64_t* d_entries, uint64_t n_entries,
+                                    uint64_t num_nodes, tribit_result* out) {
+  if (!c || (!d_entries && n_entries)) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    tb::PrepInput in;
+    in.entries = d_entries;
+    in.E = n_entries;
+    in.n = num_nodes;
+    in.order = c->opts.order;
+    run_call(c, in, nullptr, nullptr, nullptr, 0, false, out);
+    if (out) fill_schedule_stats(c, out);
+  });
+}
+
+tribit_status tribit_launch_count(tribit_context* c) {
+  if (!c) return TRIBIT_ERR_INVALID_ARGUMENT;
+  if (!c->prepared) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    tb::CountConfig cfg;
+    cfg.num_sms = c->num_sms;
+    cfg.ctas_per_sm = c->opts.ctas_per_sm;
+    c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
+  });
+}
+
+tribit_status tribit_read_count(tribit_context* c, tribit_result* out) {
+  if (!c || !c->prepared) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    TB_CUDA(cudaMemcpyAsync(c->h_stats, c->prep.stats, sizeof(tb::DeviceStats), cudaMemcpyDeviceToHost, c->st));
+    TB_CUDA(cudaStreamSynchronize(c->st));
+    TB_CUDA(cudaGetLastError());
+    if (c->h_stats->err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
+    if (out) {
+      std::memset(out, 0, sizeof *out);
+      out->triangles = c->h_stats->triangles;
+      out->num_nodes = c->prep.n;
+      out->entries = c->prep.E;
+      out->edges = c->h_stats->edges;
+      out->blocks_of_threads = c->launch.ctas;
+      out->count_kernels = c->launch.kernels;
+      fill_schedule_stats(c, out);
+    }
+  });
+}
+
+tribit_status tribit_count_mtx(tribit_context* c, const char* path, tribit_result* out) {
+  if (!c || !path) return TRIBIT_ERR_INVALID_ARGUMENT;
+  uint64_t n = 0, ne = 0;
+  uint64_t* e = nullptr;
+  tribit_status s = tribit_read_mtx(path, &n, &e, &ne);
+  if (s != TRIBIT_OK) return s;
+  s = tribit_count_edges(c, e, ne, n, out);
+  tribit_free_host(e);
+  return s;
+}
+
+tribit_status tribit_count_batch(tribit_context* c, const uint64_t* entries, const uint64_t* entry_offsets,
+                                 const uint32_t* num_nodes, uint32_t num_graphs, uint64_t* triangles_out,
+                                 tribit_result* out) {
+  if (!c || !entry_offsets || !num_nodes || !triangles_out || num_graphs == 0) return TRIBIT_ERR_INVALID_ARGUMENT;
+  if (entry_offsets[0] != 0) return TRIBIT_ERR_INVALID_ARGUMENT;
+  for (uint32_t g = 0; g < num_graphs; ++g)
+    if (entry_offsets[g + 1] < entry_offsets[g]) return TRIBIT_ERR_INVALID_ARGUMENT;
+  if (!entries && entry_offsets[num_graphs]) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    std::vector<uint64_t> voff(num_graphs + 1, 0);
+    for (uint32_t g = 0; g < num_graphs; ++g) voff[g + 1] = voff[g] + num_nodes[g];
+    tb::PrepInput in;
+    in.E = entry_offsets[num_graphs];
+    in.n = voff[num_graphs];
+    in.order = c->opts.order;
+    in.G = num_graphs;
+    static const uint64_t dummy = 0;
+    run_call(c, in, entries ? entries : &dummy, entry_offsets, voff.data(), num_graphs, true, out);
+    DeviceGuard dg(c->device);
+    TB_CUDA(cudaMemcpyAsync(triangles_out, c->per_graph, num_graphs * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->st));
+    TB_CUDA(cudaStreamSynchronize(c->st));
+    if (out) fill_schedule_stats(c, out);
+  });
+}
+
+}  // extern "C"

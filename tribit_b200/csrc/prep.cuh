@@ -1,0 +1,68 @@
+// GPU preprocessing: raw entries -> oriented, deduplicated CSR plus the
+// bit-packed 32-column block rows the counting kernels read.
+//
+// Replaces count_triangles' preprocessing (tribit.cu:666-758): the
+// reference sorts the full 64-bit words with CUB, builds separate L and U bit
+// matrices with two more 64-bit pair sorts and reduce-by-key, and syncs with
+// the host five times. Here one sort of compact keys gives both the CSR and
+// the bit rows, and nothing reads back to the host until the final count.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "arena.h"
+#include "common.cuh"
+
+namespace tb {
+
+// Device view of a prepared graph, in rank space (vertex r = the r-th vertex
+// of the chosen order). Row u holds N+(u) = neighbours of higher rank.
+struct GraphView {
+  uint32_t n;                     // vertices
+  const uint64_t* rp;             // n + 1 words: (row_ptr << 32) | brow_ptr
+  const uint32_t* col;            // N+(u), ascending, at [row_ptr[u], row_ptr[u+1])
+  const uint64_t* bent;           // bit rows: (block << 32) | mask, ascending block,
+                                  // at [brow_ptr[u], brow_ptr[u+1]); bit (w & 31) of
+                                  // block w >> 5 is set iff w in N+(u)
+  const uint32_t* graph_of_rank;  // batch mode: graph id of each rank, else null
+};
+
+__device__ __forceinline__ uint32_t rp_row(uint64_t w) { return (uint32_t)(w >> 32); }
+__device__ __forceinline__ uint32_t rp_blk(uint64_t w) { return (uint32_t)w; }
+
+// Counters the device writes and the host reads back once per call.
+struct DeviceStats {
+  unsigned long long triangles;
+  unsigned long long edges;        // undirected edges after dedup (m)
+  unsigned long long blocks;       // bit-row entries (nb)
+  unsigned int err;                // kErr* flags
+  unsigned int pad;
+  unsigned int cursor[8];          // work cursors of the counting kernels
+  unsigned int overflow[8];        // overflow-list lengths
+};
+
+struct PrepInput {
+  const uint64_t* entries = nullptr;  // device, E words (a << 32) | b
+  uint64_t E = 0;
+  uint64_t n = 0;                     // vertices (sum over graphs in batch mode)
+  int order = TRIBIT_ORDER_DEGREE;
+  // batch mode (G > 0): graph g owns entries [eoff[g], eoff[g+1]) with local
+  // ids in [0, voff[g+1] - voff[g]); its vertices are voff[g] + local id.
+  uint32_t G = 0;
+  const uint64_t* eoff = nullptr;  // device, G + 1
+  const uint64_t* voff = nullptr;  // device, G + 1
+};
+
+struct Prepared {
+  GraphView view{};
+  DeviceStats* stats = nullptr;  // device
+  uint32_t* rank = nullptr;      // id -> rank
+  uint64_t n = 0;
+  uint64_t E = 0;
+};
+
+// Lays out (measuring arena) or lays out and launches (real arena) the whole
+// preprocessing pipeline on stream st. Stats are zeroed here.
+void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* out);
+
+}  // namespace tb
