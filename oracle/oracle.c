@@ -426,6 +426,30 @@ static uint32_t lower_mask(const uint64_t* lptr, const uint32_t* lcol, uint32_t 
   return m;
 }
 
+/* Only the work decomposition of the reference (compute_n_blocks_per_row
+ * tribit.cu:645-654, total_num_blocks tribit.cu:758): sum over U entries
+ * (u, rb) of ceil(neighbours of u in blocks >= rb / 32) warps, 4 warps a CTA.
+ * entries must be folded, deduplicated and (c, r)-sorted (oracle_fold_dedup). */
+uint64_t oracle_tribit_blocks(const uint64_t* e, uint64_t m) {
+  uint64_t warps = 0, i = 0;
+  while (i < m) {
+    uint32_t c = (uint32_t)(e[i] >> 32);
+    uint64_t j = i;
+    while (j < m && (uint32_t)(e[j] >> 32) == c) j++;
+    uint64_t du = j - i;
+    if (du >= 2) {
+      uint64_t k = i;
+      while (k < j) {
+        uint32_t rb = (uint32_t)e[k] / 32;
+        warps += (j - k + 31) / 32;
+        while (k < j && (uint32_t)e[k] / 32 == rb) k++;
+      }
+    }
+    i = j;
+  }
+  return (warps + 3) / 4;
+}
+
 uint64_t oracle_count_tribit(const uint64_t* entries, uint64_t n_entries, uint64_t n, uint64_t* blocks_of_threads) {
   uint64_t* e = (uint64_t*)malloc((n_entries ? n_entries : 1) * sizeof(uint64_t));
   memcpy(e, entries, n_entries * sizeof(uint64_t));

@@ -72,6 +72,10 @@ uint64_t oracle_count_entries(const uint64_t* entries, uint64_t n_entries, uint6
  * and medium graphs. *blocks_of_threads receives ceil(total_warps / 4). */
 uint64_t oracle_count_tribit(const uint64_t* entries, uint64_t n_entries, uint64_t n, uint64_t* blocks_of_threads);
 
+/* The reference's CTA count alone (ceil(total warps / 4), tribit.cu:758) for
+ * folded, deduplicated, sorted edges; cheap at any size. */
+uint64_t oracle_tribit_blocks(const uint64_t* edges, uint64_t m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,3 +85,28 @@ def test_row_counts_sum():
     rows = g.row_counts()
     t, _ = g.count(threads=4)
     assert int(rows.sum()) == t == oracle.count(e, 1 << 11)[0]
+
+
+REF = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_counts.json")))
+
+
+@pytest.mark.parametrize("rec", [r for r in REF if r["name"] in {c["name"] for c in GOLDEN}], ids=lambda r: r["name"])
+def test_reference_binary_output_pins_oracle(rec):
+    """What the reference binary printed on a B200 equals the oracle's count and
+    its restatement of the reference's work decomposition."""
+    want = [c for c in GOLDEN if c["name"] == rec["name"]][0]
+    assert rec["status"] == "ok" and rec["cuda"] == "No cuda error detected"
+    assert rec["triangles"] == want["triangles"]
+    assert rec["blocks_of_threads"] == want["reference_blocks_of_threads"]
+
+
+def test_reference_binary_rmat18_pins_oracle():
+    import ctypes
+    rec = [r for r in REF if r["name"] == "rmat_s18"][0]
+    e = tb.gen_rmat(18, 16, seed=rec["params"]["seed"])
+    t, _ = oracle.count(e, 1 << 18)
+    assert t == rec["triangles"]
+    f = oracle.fold_dedup(e)
+    oracle._lib.oracle_tribit_blocks.restype = ctypes.c_uint64
+    oracle._lib.oracle_tribit_blocks.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+    assert oracle._lib.oracle_tribit_blocks(f.ctypes.data, f.size) == rec["blocks_of_threads"]
