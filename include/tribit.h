@@ -139,6 +139,30 @@ tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, c
                                  const uint32_t* num_nodes, uint32_t num_graphs, uint64_t* triangles_out,
                                  tribit_result* out);
 
+/* ---- counting without device allocation ---------------------------------- */
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory while they count: a process whose framework owns the device memory
+ * through its own allocator or a pool reserved up front (as the reference
+ * reserves 95% of free memory at start-up), or a latency-bound loop that must
+ * not pay the implicit synchronisation of cudaMalloc / cudaFree.
+ * Counts the graph in d_entries (device memory, zipped words as for
+ * tribit_count_edges; degree order, plain dispatch) on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream), taking every intermediate
+ * buffer from one fixed scratch array compiled into the library
+ * (tribit_noalloc_scratch_bytes() = 32 MiB, held on each device that loads it
+ * until exit). Allocates no device or host memory and needs no context.
+ * Asynchronous: when the stream reaches the end of the work, d_result (device,
+ * 4 x uint64) holds [0] triangles, [1] undirected edges, [2] error flags (bit 0:
+ * an entry named a vertex >= num_nodes, the count is then invalid), [3] 0.
+ * Returns TRIBIT_ERR_TOO_LARGE, launching nothing, for a graph whose buffers
+ * do not fit the scratch array (roughly 36 bytes per entry + 40 per vertex).
+ * The first call on a device looks up the array's device address: make it
+ * before capturing stream work on that device. All calls share the array, so
+ * calls whose GPU work overlaps race: order them on one stream. */
+tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, uint64_t n_entries, uint64_t num_nodes,
+                                         uint64_t* d_result, void* stream);
+uint64_t tribit_noalloc_scratch_bytes(void);
+
 /* ---- learned dispatcher ------------------------------------------------- */
 /* Loads MLP weights (16 -> 64 -> 64 -> 3) written by tribit_model_save. */
 tribit_status tribit_model_load(tribit_context* ctx, const char* path);

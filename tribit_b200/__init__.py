@@ -79,6 +79,8 @@ _decl("tribit_free_host", None, _p)
 _decl("tribit_count_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
 _decl("tribit_count_batch", ctypes.c_int, _p, _p, _p, _p, _u32, _p, ctypes.POINTER(_Result))
 _decl("tribit_model_load", ctypes.c_int, _p, ctypes.c_char_p)
+_decl("tribit_count_edges_noalloc", ctypes.c_int, _p, _u64, _u64, _p, _p)
+_decl("tribit_noalloc_scratch_bytes", _u64)
 _decl("tribit_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, _p)
 _decl("tribit_gen_er", ctypes.c_int, _u32, _u64, _u64, _p)
 _decl("tribit_gen_chung_lu", ctypes.c_int, _u32, _u64, ctypes.c_double, ctypes.c_double, _u64, _p)
@@ -207,6 +209,18 @@ class Counter:
         _check(lib.tribit_count_batch(self._h, e.ctypes.data if e.size else None, off.ctypes.data, nn.ctypes.data, g,
                                       out.ctypes.data, ctypes.byref(r)), self._h)
         return out, Result._from(r)
+
+
+def count_edges_noalloc(entries_ptr: int, n_entries: int, num_nodes: int, result_ptr: int, stream_ptr: int = 0):
+    """tribit_count_edges_noalloc: counts the graph at device address entries_ptr
+    without allocating anything, for callers whose device memory is owned by
+    someone else (a framework allocator or a pool reserved up front) or who
+    cannot afford cudaMalloc's implicit synchronisation. All scratch comes
+    from one fixed 32 MiB device array inside the library. Asynchronous on
+    stream_ptr: result_ptr (4 x uint64 in device memory) receives
+    [triangles, edges, error flags, 0]. Raises TribitError (status 6) for a
+    graph too large for the scratch array."""
+    _check(lib.tribit_count_edges_noalloc(entries_ptr, n_entries, int(num_nodes), result_ptr, stream_ptr or None))
 
 
 def read_mtx(path: str):

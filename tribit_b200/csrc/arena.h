@@ -32,6 +32,8 @@ class Arena {
 
   void reserve(size_t bytes) {
     if (bytes <= cap_) return;
+    if (base_ && !owned_)
+      throw StatusError(TRIBIT_ERR_TOO_LARGE, "graph needs more scratch than the fixed device buffer holds");
     release();
     size_t want = bytes + (bytes >> 4);  // headroom so slightly larger calls reuse it
     cudaError_t e = cudaMalloc(&base_, want);
@@ -56,16 +58,28 @@ class Arena {
   bool measuring() const { return measuring_; }
 
   void release() {
-    if (base_) cudaFree(base_);
+    if (base_ && owned_) cudaFree(base_);
     base_ = nullptr;
     cap_ = 0;
+    owned_ = true;
   }
+
+  // Hands out slices of caller-owned device memory instead of allocating:
+  // reserve() then only checks that the layout fits in `bytes`.
+  void attach(void* base, size_t bytes) {
+    release();
+    base_ = base;
+    cap_ = bytes;
+    owned_ = false;
+  }
+  bool attached() const { return !owned_; }
 
  private:
   void* base_ = nullptr;
   size_t cap_ = 0;
   size_t off_ = 0;
   bool measuring_ = false;
+  bool owned_ = true;
 };
 
 }  // namespace tb
