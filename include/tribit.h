@@ -163,9 +163,40 @@ tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, uint64_t n_e
                                          uint64_t* d_result, void* stream);
 uint64_t tribit_noalloc_scratch_bytes(void);
 
-/* ---- learned dispatcher ------------------------------------------------- */
-/* Loads MLP weights (16 -> 64 -> 64 -> 3) written by tribit_model_save. */
+/* ---- learned dispatcher (no counterpart in the reference) ----------------- */
+/* A 16 -> 64 -> 64 -> 3 MLP (ReLU; BF16 weights, FP32 activations and
+ * accumulation) maps the 16 features of a 32-row block to the predicted
+ * log2(1 + SM cycles) each counting variant spends on it; learned dispatch
+ * runs every row block on the variant with the smallest prediction. It only
+ * schedules: counts are exact under any dispatcher. */
+uint32_t tribit_model_num_params(void); /* 5443 */
+/* Fresh model: weights uniform in +-sqrt(6 / fan_in) from `seed`, zero biases;
+ * norm = in_mean[16], in_std[16], out_mean[3], out_std[3]. */
+tribit_status tribit_model_init(tribit_context* ctx, uint64_t seed, const float* norm);
 tribit_status tribit_model_load(tribit_context* ctx, const char* path);
+tribit_status tribit_model_save(tribit_context* ctx, const char* path);
+/* effective != 0: the parameters as the kernels use them (weights rounded to BF16). */
+tribit_status tribit_model_get_params(tribit_context* ctx, float* out, int effective);
+tribit_status tribit_model_set_params(tribit_context* ctx, const float* in);
+/* y[rows x 3] = predicted log2(1 + cycles) per variant for features x[rows x 16]. */
+tribit_status tribit_model_predict(tribit_context* ctx, const float* x, uint64_t rows, float* y);
+/* Gradient of the mean squared error on normalised targets over all rows
+ * (one batch), with respect to the effective parameters; *loss receives it. */
+tribit_status tribit_model_gradients(tribit_context* ctx, const float* x, const float* y, uint64_t rows, float* grad,
+                                     float* loss);
+/* Adam (0.9, 0.999, 1e-8) on the GPU; *loss receives the last epoch's mean loss. */
+tribit_status tribit_model_train(tribit_context* ctx, const float* x, const float* y, uint64_t rows, uint32_t epochs,
+                                 uint32_t batch, float lr, uint64_t seed, float* loss);
+
+/* ---- per-row-block data for the dispatcher (after tribit_prepare_device) -- */
+/* Features of every 32-row block (num_row_blocks x 16 floats; out may be NULL
+ * to query the count). */
+tribit_status tribit_block_features(tribit_context* ctx, float* out, uint64_t cap, uint64_t* num_row_blocks);
+/* Counts with every row block on `variant` (TRIBIT_VARIANT_*) and records the
+ * SM cycles each row block's pieces took (cycles_out[num_row_blocks]);
+ * *triangles receives the count, which equals the normal one. */
+tribit_status tribit_block_times(tribit_context* ctx, int variant, float* cycles_out, uint64_t cap,
+                                 uint64_t* triangles);
 
 /* ---- synthetic graphs (host, seeded, thread-count independent) ---------- */
 tribit_status tribit_gen_rmat(int scale, uint64_t edge_factor, double a, double b, double c, uint64_t seed,

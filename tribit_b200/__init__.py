@@ -79,6 +79,17 @@ _decl("tribit_free_host", None, _p)
 _decl("tribit_count_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
 _decl("tribit_count_batch", ctypes.c_int, _p, _p, _p, _p, _u32, _p, ctypes.POINTER(_Result))
 _decl("tribit_model_load", ctypes.c_int, _p, ctypes.c_char_p)
+_decl("tribit_model_save", ctypes.c_int, _p, ctypes.c_char_p)
+_decl("tribit_model_num_params", _u32)
+_decl("tribit_model_init", ctypes.c_int, _p, _u64, _p)
+_decl("tribit_model_get_params", ctypes.c_int, _p, _p, ctypes.c_int)
+_decl("tribit_model_set_params", ctypes.c_int, _p, _p)
+_decl("tribit_model_predict", ctypes.c_int, _p, _p, _u64, _p)
+_decl("tribit_model_gradients", ctypes.c_int, _p, _p, _p, _u64, _p, ctypes.POINTER(ctypes.c_float))
+_decl("tribit_model_train", ctypes.c_int, _p, _p, _p, _u64, _u32, _u32, ctypes.c_float, _u64,
+      ctypes.POINTER(ctypes.c_float))
+_decl("tribit_block_features", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
+_decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POINTER(_u64))
 _decl("tribit_count_edges_noalloc", ctypes.c_int, _p, _u64, _u64, _p, _p)
 _decl("tribit_noalloc_scratch_bytes", _u64)
 _decl("tribit_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, _p)
@@ -166,6 +177,63 @@ class Counter:
 
     def load_model(self, path: str):
         _check(lib.tribit_model_load(self._h, path.encode()), self._h)
+
+    # -- learned dispatcher ------------------------------------------------
+    def model_init(self, norm, seed: int = 1):
+        nrm = np.ascontiguousarray(norm, dtype=np.float32)
+        assert nrm.size == 38
+        _check(lib.tribit_model_init(self._h, seed, nrm.ctypes.data), self._h)
+
+    def save_model(self, path: str):
+        _check(lib.tribit_model_save(self._h, path.encode()), self._h)
+
+    def model_params(self, effective: bool = False) -> np.ndarray:
+        out = np.zeros(lib.tribit_model_num_params(), dtype=np.float32)
+        _check(lib.tribit_model_get_params(self._h, out.ctypes.data, int(effective)), self._h)
+        return out
+
+    def set_model_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib.tribit_model_set_params(self._h, p.ctypes.data), self._h)
+
+    def model_predict(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 16)
+        y = np.zeros((x.shape[0], 3), dtype=np.float32)
+        _check(lib.tribit_model_predict(self._h, x.ctypes.data, x.shape[0], y.ctypes.data), self._h)
+        return y
+
+    def model_gradients(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 16)
+        y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1, 3)
+        g = np.zeros(lib.tribit_model_num_params(), dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib.tribit_model_gradients(self._h, x.ctypes.data, y.ctypes.data, x.shape[0], g.ctypes.data,
+                                          ctypes.byref(loss)), self._h)
+        return g, loss.value
+
+    def model_train(self, x, y, epochs: int = 10, batch: int = 4096, lr: float = 1e-3, seed: int = 1) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 16)
+        y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1, 3)
+        loss = ctypes.c_float()
+        _check(lib.tribit_model_train(self._h, x.ctypes.data, y.ctypes.data, x.shape[0], epochs, batch, lr, seed,
+                                      ctypes.byref(loss)), self._h)
+        return loss.value
+
+    def block_features(self) -> np.ndarray:
+        nrb = _u64()
+        _check(lib.tribit_block_features(self._h, None, 0, ctypes.byref(nrb)), self._h)
+        out = np.zeros((nrb.value, 16), dtype=np.float32)
+        _check(lib.tribit_block_features(self._h, out.ctypes.data, out.size, ctypes.byref(nrb)), self._h)
+        return out
+
+    def block_times(self, variant: str):
+        nrb = _u64()
+        _check(lib.tribit_block_features(self._h, None, 0, ctypes.byref(nrb)), self._h)
+        out = np.zeros(nrb.value, dtype=np.float32)
+        tri = _u64()
+        _check(lib.tribit_block_times(self._h, VARIANTS.index(variant), out.ctypes.data, out.size,
+                                      ctypes.byref(tri)), self._h)
+        return out, tri.value
 
     def count_edges(self, entries, num_nodes: int) -> Result:
         e = _entries(entries)

@@ -6,64 +6,14 @@
 #include <string>
 #include <vector>
 
-#include "arena.h"
-#include "common.cuh"
-#include "count.cuh"
-#include "prep.cuh"
-#include "tribit.h"
-
-struct tribit_context {
-  tribit_options opts{};
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t own = nullptr;
-  cudaStream_t st = nullptr;
-  tb::Arena arena;
-  tb::Prepared prep{};
-  tb::Schedule sched{};
-  unsigned long long* per_graph = nullptr;
-  bool prepared = false;
-  tb::LaunchInfo launch{};
-  cudaEvent_t ev[6] = {};
-  tb::DeviceStats* h_stats = nullptr;  // pinned
-  std::string err;
-};
+#include "context.h"
 
 namespace {
 
 using tb::CudaError;
+using tb::DeviceGuard;
 using tb::StatusError;
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-template <typename F>
-tribit_status guarded(tribit_context* ctx, F&& body) {
-  try {
-    body();
-    return TRIBIT_OK;
-  } catch (const StatusError& e) {
-    if (ctx) ctx->err = e.what();
-    return e.status;
-  } catch (const CudaError& e) {
-    if (ctx) ctx->err = e.what();
-    return e.code == cudaErrorMemoryAllocation ? TRIBIT_ERR_OUT_OF_MEMORY : TRIBIT_ERR_CUDA;
-  } catch (const std::bad_alloc&) {
-    if (ctx) ctx->err = "host allocation failed";
-    return TRIBIT_ERR_OUT_OF_MEMORY;
-  } catch (const std::exception& e) {
-    if (ctx) ctx->err = e.what();
-    return TRIBIT_ERR_INTERNAL;
-  }
-}
+using tb::guarded;
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
@@ -99,7 +49,7 @@ void layout(tribit_context* c, bool measure, const tb::PrepInput& in, bool stage
   // Measuring: walk the same takes prepare_graph / take_schedule will do.
   tb::Prepared tmp;
   tb::prepare_graph(ar, pin, c->st, &tmp);
-  (void)tb::take_schedule(ar, in.n);
+  (void)tb::take_schedule(ar, in.n, in.E);
 }
 
 // Runs preprocessing + schedule (+ counting when count == true) for one input.
@@ -127,8 +77,8 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
     pin.voff = L.voff;
   }
   tb::prepare_graph(c->arena, pin, st, &c->prep);
-  c->sched = tb::take_schedule(c->arena, in.n);
-  tb::build_schedule(c->prep.view, c->sched, c->opts.dispatch, nullptr, st);
+  c->sched = tb::take_schedule(c->arena, in.n, in.E);
+  tb::apply_dispatch(c, st);
   c->per_graph = L.per_graph;
   c->prepared = true;
   TB_CUDA(cudaEventRecord(c->ev[2], st));
@@ -246,6 +196,9 @@ void tribit_destroy(tribit_context* c) {
     DeviceGuard dg(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     c->arena.release();
+    c->train_arena.release();
+    c->timing_arena.release();
+    tb::model_free(c->model);
     for (auto& e : c->ev)
       if (e) cudaEventDestroy(e);
     if (c->h_stats) cudaFreeHost(c->h_stats);

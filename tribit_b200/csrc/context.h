@@ -1,0 +1,74 @@
+// The tribit_context behind the C-ABI handle, shared by the C-ABI sources.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <new>
+#include <string>
+
+#include "arena.h"
+#include "common.cuh"
+#include "count.cuh"
+#include "model.cuh"
+#include "prep.cuh"
+#include "tribit.h"
+
+struct tribit_context {
+  tribit_options opts{};
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t st = nullptr;
+  tb::Arena arena;
+  tb::Prepared prep{};
+  tb::Schedule sched{};
+  unsigned long long* per_graph = nullptr;
+  bool prepared = false;
+  tb::LaunchInfo launch{};
+  cudaEvent_t ev[6] = {};
+  tb::DeviceStats* h_stats = nullptr;  // pinned
+  tb::DeviceModel model{};
+  tb::Arena train_arena;               // training batches and activations
+  tb::Arena timing_arena;              // per-row-block cycle counters
+  std::string err;
+};
+
+namespace tb {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Runs body, mapping library exceptions to statuses (and the message into
+// ctx->err); nothing escapes an extern "C" function.
+template <typename F>
+tribit_status guarded(tribit_context* ctx, F&& body) {
+  try {
+    body();
+    return TRIBIT_OK;
+  } catch (const StatusError& e) {
+    if (ctx) ctx->err = e.what();
+    return e.status;
+  } catch (const CudaError& e) {
+    if (ctx) ctx->err = e.what();
+    return e.code == cudaErrorMemoryAllocation ? TRIBIT_ERR_OUT_OF_MEMORY : TRIBIT_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    if (ctx) ctx->err = "host allocation failed";
+    return TRIBIT_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->err = e.what();
+    return TRIBIT_ERR_INTERNAL;
+  }
+}
+
+// Rebuilds the context's schedule for its dispatch mode (learned mode runs the
+// MLP over full features).
+void apply_dispatch(tribit_context* c, cudaStream_t st);
+
+}  // namespace tb

@@ -1,11 +1,15 @@
 // Counting kernels; see count.cuh.
 //
-// Work unit: a 32-row block of the oriented graph (ranks 32*rb .. 32*rb+31).
-// Each variant kernel is persistent (grid = SMs x CTAs/SM) and pulls row
-// blocks of its own list, highest rank first, from a device cursor. A row that
-// does not fit a warp's shared-memory slice is deferred to a CTA-wide pass,
-// and a row too large for that to a global-memory pass, so every row of every
-// list is counted exactly once whatever its size.
+// A piece is (row u, neighbours [s, min(s + 64, d+(u)))). A warp that takes a
+// piece of u loads u's row into a per-warp shared-memory structure -- a
+// bucketed hash of u's 32-column bit blocks (bitmap variant) or u's sorted
+// neighbour list (merge variant) -- reusing it when its next piece is of the
+// same row, then visits every item of every neighbour v of the piece: v's bit
+// blocks (bitmap) or v's neighbours (merge), each looked up in u's structure.
+// Neighbours with long lists are swept by all 32 lanes; short lists are
+// flattened across lanes. Rows whose structure does not fit a warp's slice go
+// whole to a CTA-wide pass, and rows too large for that to a global-memory
+// pass, so every piece of every list is counted exactly once.
 #include "count.cuh"
 #include "scan.cuh"
 
@@ -14,139 +18,251 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kWarpsPerCta = 8;
-constexpr int kWarpSlots = 512;                        // 8-byte words of shared memory per warp
-constexpr uint32_t kWarpMaxBlocks = kWarpSlots / 2;    // bitmap rows up to this many bit blocks
-constexpr uint32_t kWarpMaxList = kWarpSlots * 2;      // merge rows up to this many neighbours
+constexpr int kWarpSlots = 512;                      // 8-byte words of shared memory per warp
+constexpr uint32_t kWarpMaxBlocks = kWarpSlots / 2;  // bitmap rows up to this many bit blocks
+constexpr uint32_t kWarpMaxList = kWarpSlots * 2;    // merge rows up to this many neighbours
 constexpr int kCtaThreads = 512;
-constexpr int kCtaLogSlots = 14;                       // 16384 slots = 128 KiB
+constexpr int kCtaLogSlots = 14;                     // 16384 slots = 128 KiB
 constexpr uint32_t kCtaMaxBlocks = (1u << kCtaLogSlots) / 2;
+constexpr uint32_t kLong = 24;                       // lists at least this long are swept by the whole warp
+constexpr uint32_t kGrab = 4;                        // pieces taken per cursor update
 constexpr uint64_t kEmptySlot = 0xFFFFFFFF00000000ull;
 
-enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5 };
+enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6 };
+constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 2;  // CTA-shared table in the same 32 KiB
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 enum { kOvfCta = 0, kOvfGlobal = 1 };
+constexpr int kTileMaxK = 64;  // bit-tile variant: at most this many column blocks (2048 columns)
 
-__device__ __forceinline__ int log2_ceil(uint32_t x) {  // smallest b with 2^b >= x
-  return x <= 1 ? 0 : 32 - __clz(x - 1);
+__device__ __forceinline__ int log2_ceil(uint32_t x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
+
+__device__ __forceinline__ uint32_t hash_bucket(uint32_t blk, int logb) {
+  return (blk * 0x9E3779B1u) >> (32 - logb);
 }
 
-__device__ __forceinline__ uint32_t hash_slot(uint32_t blk, int logsz) { return (blk * 0x9E3779B1u) >> (32 - logsz); }
+// ---- bucketed hash of a row's bit blocks -----------------------------------
+// 2^logb buckets of two 8-byte slots, (block << 32) | mask; a bucket's second
+// slot fills only after its first, buckets probe linearly, and the table is at
+// most half full, so every lookup ends at a bucket with an empty second slot.
 
-// Open-addressing table of one row's bit blocks: slot = (block << 32) | mask,
-// linear probing, at most half full, so every probe sequence ends.
-__device__ __forceinline__ void table_clear(uint64_t* tbl, int logsz, int tid, int nthreads) {
-  for (int s = tid; s < (1 << logsz); s += nthreads) tbl[s] = kEmptySlot;
+__device__ __forceinline__ void table_clear(uint64_t* t, int logb, int tid, int nth) {
+  for (int s = tid; s < (2 << logb); s += nth) t[s] = kEmptySlot;
 }
 
-__device__ __forceinline__ void table_insert(uint64_t* tbl, int logsz, const uint64_t* __restrict__ bent, uint32_t bs,
-                                             uint32_t be, int tid, int nthreads) {
-  const uint32_t m = (1u << logsz) - 1u;
-  for (uint32_t k = bs + tid; k < be; k += nthreads) {
-    uint64_t e = bent[k];
-    uint32_t h = hash_slot((uint32_t)(e >> 32), logsz);
-    while (atomicCAS(reinterpret_cast<unsigned long long*>(tbl + h), kEmptySlot, e) != kEmptySlot) h = (h + 1) & m;
+__device__ __forceinline__ void table_insert(uint64_t* t, int logb, const uint64_t* __restrict__ bent, uint32_t bs,
+                                             uint32_t be, int tid, int nth) {
+  const uint32_t m = (1u << logb) - 1u;
+  for (uint32_t k = bs + tid; k < be; k += nth) {
+    const uint64_t e = bent[k];
+    uint32_t b = hash_bucket((uint32_t)(e >> 32), logb);
+    for (;;) {
+      unsigned long long* slot = reinterpret_cast<unsigned long long*>(t + 2 * b);
+      if (atomicCAS(slot, kEmptySlot, e) == kEmptySlot) break;
+      if (atomicCAS(slot + 1, kEmptySlot, e) == kEmptySlot) break;
+      b = (b + 1) & m;
+    }
   }
 }
 
-__device__ __forceinline__ uint32_t table_find(const uint64_t* tbl, int logsz, uint32_t blk) {
-  const uint32_t m = (1u << logsz) - 1u;
-  uint32_t h = hash_slot(blk, logsz);
+__device__ __forceinline__ uint32_t table_find(const uint64_t* t, int logb, uint32_t blk) {
+  const uint32_t m = (1u << logb) - 1u;
+  uint32_t b = hash_bucket(blk, logb);
   for (;;) {
-    uint64_t x = tbl[h];
-    uint32_t k = (uint32_t)(x >> 32);
-    if (k == blk) return (uint32_t)x;
-    if (k == 0xFFFFFFFFu) return 0u;
-    h = (h + 1) & m;
+    const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(t + 2 * b);
+    if ((uint32_t)(x.x >> 32) == blk) return (uint32_t)x.x;
+    if ((uint32_t)(x.y >> 32) == blk) return (uint32_t)x.y;
+    if ((uint32_t)(x.y >> 32) == 0xFFFFFFFFu) return 0u;
+    b = (b + 1) & m;
   }
 }
 
-// Visits, for the neighbours N+(u)[c] with c in [rs, re) taken in chunks of 32
-// (chunk0, chunk0 + step, ...), every item of each neighbour's list -- its bit
-// blocks (Blocks) or its neighbour ids -- spreading the flattened items of a
-// chunk over the warp's lanes. probe(item_index, neighbour_slot) returns the
-// matches it found. Must be called by all 32 lanes.
-template <bool Blocks, class Probe>
-__device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t rs, uint32_t re, uint32_t chunk0,
-                                          uint32_t step, Probe&& probe) {
+// Buckets for a row of nb bit blocks: at least nb (load <= 1/2), at least 16.
+__device__ __forceinline__ int table_logb(uint32_t nb) { return max(4, log2_ceil(nb)); }
+
+struct BitmapProbe {
+  const uint64_t* t;
+  int logb;
+  uint32_t bmin, bmax;
+  __device__ __forceinline__ uint32_t operator()(uint64_t e) const {
+    const uint32_t blk = (uint32_t)(e >> 32);
+    if (blk < bmin || blk > bmax) return 0u;
+    return (uint32_t)__popc((uint32_t)e & table_find(t, logb, blk));
+  }
+};
+
+// ---- the neighbour sweep ---------------------------------------------------
+// For neighbours N+(u)[c] with c in [cs, ce) in chunks of 32 (chunk0,
+// chunk0 + step, ...) visits every item of each neighbour's list: its bit
+// blocks (Blocks) or its neighbour ids. item(k, c) returns the matches of item
+// index k of neighbour slot c. Must be called by all 32 lanes of the warp.
+
+template <bool Blocks, class Item>
+__device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
+                                          uint32_t step, const Item& item) {
   const uint32_t lane = threadIdx.x & 31;
   uint64_t acc = 0;
-  for (uint32_t c = rs + chunk0 * 32; c < re; c += step * 32) {
-    uint32_t j = c + lane;
+  for (uint32_t c = cs + chunk0 * 32; c < ce; c += step * 32) {
+    const uint32_t j = c + lane;
     uint32_t ib = 0, il = 0;
-    if (j < re) {
-      uint32_t v = g.col[j];
-      uint64_t a = g.rp[v], b = g.rp[v + 1];
-      if (Blocks) {
-        ib = rp_blk(a);
-        il = rp_blk(b) - ib;
-      } else {
-        ib = rp_row(a);
-        il = rp_row(b) - ib;
+    if (j < ce) {
+      const uint32_t v = g.col[j];
+      const uint64_t a = g.rp[v], b = g.rp[v + 1];
+      ib = Blocks ? rp_blk(a) : rp_row(a);
+      il = (Blocks ? rp_blk(b) : rp_row(b)) - ib;
+    }
+    // Long lists: one neighbour at a time, all lanes, two items per lane in flight.
+    uint32_t longm = __ballot_sync(kFull, il >= kLong);
+    while (longm) {
+      const int s = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const uint32_t sb = __shfl_sync(kFull, ib, s), sl = __shfl_sync(kFull, il, s);
+      const uint32_t cj = c + s;
+      for (uint32_t k = lane; k < sl; k += 64) {
+        const uint32_t k2 = k + 32;
+        const uint32_t r0 = item(sb + k, cj);
+        const uint32_t r1 = k2 < sl ? item(sb + k2, cj) : 0u;
+        acc += r0 + r1;
       }
     }
-    uint32_t incl = warp_inclusive_sum(il);
-    uint32_t total = __shfl_sync(kFull, incl, 31);
-    uint32_t excl = incl - il;
+    // Short lists: flattened over lanes; the owner of item t is the lane
+    // whose inclusive prefix first exceeds t.
+    const uint32_t sl = il >= kLong ? 0u : il;
+    const uint32_t incl = warp_inclusive_sum(sl);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t excl = incl - sl;
     for (uint32_t base = 0; base < total; base += 32) {
-      uint32_t t = base + lane;
+      const uint32_t t = base + lane;
       uint32_t s = 0;
 #pragma unroll
       for (uint32_t st = 16; st >= 1; st >>= 1) {
-        uint32_t x = __shfl_sync(kFull, incl, s + st - 1);
+        const uint32_t x = __shfl_sync(kFull, incl, s + st - 1);
         if (x <= t) s += st;
       }
-      uint32_t sb = __shfl_sync(kFull, ib, s);
-      uint32_t se = __shfl_sync(kFull, excl, s);
-      if (t < total) acc += probe(sb + (t - se), c + s);
+      const uint32_t sb = __shfl_sync(kFull, ib, s);
+      const uint32_t se = __shfl_sync(kFull, excl, s);
+      if (t < total) acc += item(sb + (t - se), c + s);
     }
   }
   return acc;
 }
 
 __device__ __forceinline__ void push_row(DeviceStats* stats, int which, uint32_t* list, uint32_t u) {
-  uint32_t i = atomicAdd(&stats->overflow[which], 1u);
+  const uint32_t i = atomicAdd(&stats->overflow[which], 1u);
   list[i] = u;
 }
 
-// ---- warp-per-row kernels (bitmap and merge variants) --------------------
+// SM cycle counter; a piece runs on one SM, so differences are meaningful.
+__device__ __forceinline__ unsigned long long cycles() { return (unsigned long long)clock64(); }
+
+// ---- warp-per-piece kernels (bitmap and merge variants) --------------------
 
 template <int V>
-__global__ void __launch_bounds__(kWarpsPerCta * 32) k_rows_warp(GraphView g, const uint32_t* __restrict__ list,
-                                                                  const uint32_t* __restrict__ list_len,
-                                                                  DeviceStats* stats, uint32_t* __restrict__ ovf_cta,
-                                                                  unsigned long long* per_graph) {
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, const uint64_t* __restrict__ pieces,
+                                                                    const uint32_t* __restrict__ piece_off,
+                                                                    DeviceStats* stats, uint32_t* __restrict__ ovf_cta,
+                                                                    unsigned long long* per_graph,
+                                                                    unsigned long long* block_ns,
+                                                                    const uint32_t* __restrict__ heavy) {
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
+  __shared__ uint32_t s_row;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* tbl = smem[w];
   uint32_t* lst = reinterpret_cast<uint32_t*>(smem[w]);
-  const uint32_t len = list_len[V];
+  const uint32_t p0 = piece_off[V], len = piece_off[V + 1] - p0;
   uint64_t acc = 0;
+  // Phase 1 (first kernel only): rows too wide for a warp's slice, one at a
+  // time per CTA, with a CTA-shared table in the same shared memory and all
+  // warps sweeping the row's neighbour chunks.
+  if (heavy) {
+    uint64_t* ctbl = &smem[0][0];
+    const uint32_t hlen = piece_off[TRIBIT_NUM_VARIANTS + 1];
+    for (;;) {
+      if (threadIdx.x == 0) {
+        const uint32_t t = atomicAdd(&stats->cursor[kCurHeavy], 1u);
+        s_row = t < hlen ? heavy[hlen - 1 - t] : kNoRow;
+      }
+      __syncthreads();
+      const uint32_t u = s_row;
+      if (u == kNoRow) break;
+      const uint64_t a = g.rp[u], b = g.rp[u + 1];
+      const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
+      if (nb > kHeavyMaxBlocks) {
+        if (threadIdx.x == 0) push_row(stats, kOvfCta, ovf_cta, u);
+        __syncthreads();
+        continue;
+      }
+      const int logb = table_logb(nb);
+      table_clear(ctbl, logb, threadIdx.x, blockDim.x);
+      __syncthreads();
+      table_insert(ctbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
+      __syncthreads();
+      const BitmapProbe probe{ctbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
+      const uint64_t racc = sweep<true>(g, rs, re, w, kWarpsPerCta,
+                                        [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+      if (per_graph) {
+        const uint64_t s = warp_sum(racc);
+        if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
+      }
+      acc += racc;
+      __syncthreads();  // the table and s_row are rewritten for the next row
+    }
+    __syncthreads();
+  }
+  uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
+  bool cur_ok = false;
+  int logb = 0;
+  uint32_t bmin = 0, bmax = 0, d = 0, last = 0;
   for (;;) {
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(&stats->cursor[kCurVariant0 + V], 1u);
-    t = __shfl_sync(kFull, t, 0);
-    if (t >= len) break;
-    const uint32_t rb = list[len - 1 - t];
-    const uint32_t u0 = rb * 32, u1 = min(u0 + 32, g.n);
-    for (uint32_t u = u0; u < u1; ++u) {
+    uint32_t t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurVariant0 + V], kGrab);
+    t0 = __shfl_sync(kFull, t0, 0);
+    if (t0 >= len) break;
+    const uint32_t t1 = min(t0 + kGrab, len);
+    for (uint32_t t = t0; t < t1; ++t) {
+      const uint64_t pc = pieces[p0 + (len - 1 - t)];
+      const uint32_t u = (uint32_t)(pc >> 32), first = (uint32_t)pc;
       const uint64_t a = g.rp[u], b = g.rp[u + 1];
       const uint32_t rs = rp_row(a), re = rp_row(b);
-      if (re - rs < 2) continue;
-      uint64_t racc = 0;
-      if (V == TRIBIT_VARIANT_MERGE) {
-        const uint32_t d = re - rs;
-        if (d > kWarpMaxList) {
-          if (lane == 0) push_row(stats, kOvfCta, ovf_cta, u);
-          continue;
-        }
-        for (uint32_t k = lane; k < d; k += 32) lst[k] = g.col[rs + k];
+      unsigned long long t_start = 0;
+      if (block_ns && lane == 0) t_start = cycles();
+      if (u != cur) {
         __syncwarp();
-        const uint32_t last = lst[d - 1];
-        racc = sweep<false>(g, rs, re, 0, 1, [&](uint32_t k, uint32_t c) -> uint32_t {
-          uint32_t x = g.col[k];
+        cur = u;
+        if (V == TRIBIT_VARIANT_MERGE) {
+          d = re - rs;
+          cur_ok = d <= kWarpMaxList;
+          if (cur_ok) {
+            for (uint32_t k = lane; k < d; k += 32) lst[k] = g.col[rs + k];
+            last = g.col[re - 1];
+          }
+        } else {
+          const uint32_t bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
+          cur_ok = nb <= kWarpMaxBlocks;
+          if (cur_ok) {
+            logb = table_logb(nb);
+            table_clear(tbl, logb, lane, 32);
+            __syncwarp();
+            table_insert(tbl, logb, g.bent, bs, be, lane, 32);
+            bmin = (uint32_t)(g.bent[bs] >> 32);
+            bmax = (uint32_t)(g.bent[be - 1] >> 32);
+          }
+        }
+        __syncwarp();
+      }
+      if (!cur_ok) {
+        // The whole row goes to the CTA pass once, from its first piece.
+        if (first == 0 && lane == 0) push_row(stats, kOvfCta, ovf_cta, u);
+        continue;
+      }
+      const uint32_t cs = rs + first, ce = min(cs + kPieceNeighbours, re);
+      uint64_t racc;
+      if (V == TRIBIT_VARIANT_MERGE) {
+        racc = sweep<false>(g, cs, ce, 0, 1, [&](uint32_t k, uint32_t c) -> uint32_t {
+          const uint32_t x = g.col[k];
           if (x > last) return 0u;
           uint32_t lo = c - rs + 1, hi = d;
           while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
+            const uint32_t mid = (lo + hi) >> 1;
             if (lst[mid] < x)
               lo = mid + 1;
             else
@@ -154,30 +270,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_rows_warp(GraphView g, co
           }
           return (lo < d && lst[lo] == x) ? 1u : 0u;
         });
-        __syncwarp();
       } else {
-        const uint32_t bs = rp_blk(a), be = rp_blk(b), nbu = be - bs;
-        if (nbu > kWarpMaxBlocks) {
-          if (lane == 0) push_row(stats, kOvfCta, ovf_cta, u);
-          continue;
-        }
-        const int logsz = max(5, log2_ceil(2 * nbu));
-        table_clear(tbl, logsz, lane, 32);
-        __syncwarp();
-        table_insert(tbl, logsz, g.bent, bs, be, lane, 32);
-        __syncwarp();
-        const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32), bmax = (uint32_t)(g.bent[be - 1] >> 32);
-        racc = sweep<true>(g, rs, re, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t {
-          uint64_t e = g.bent[k];
-          uint32_t blk = (uint32_t)(e >> 32);
-          if (blk < bmin || blk > bmax) return 0u;
-          return (uint32_t)__popc((uint32_t)e & table_find(tbl, logsz, blk));
-        });
-        __syncwarp();
+        const BitmapProbe probe{tbl, logb, bmin, bmax};
+        racc = sweep<true>(g, cs, ce, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
       }
       if (per_graph) {
-        uint64_t s = warp_sum(racc);
+        const uint64_t s = warp_sum(racc);
         if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
+      }
+      if (block_ns) {
+        __syncwarp();
+        if (lane == 0) atomicAdd(&block_ns[u >> 5], cycles() - t_start);
       }
       acc += racc;
     }
@@ -186,7 +289,201 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_rows_warp(GraphView g, co
   if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
-// ---- CTA-per-row pass for rows deferred by the warp kernels --------------
+// ---- bit-tile MMA variant -----------------------------------------------------
+// One warp per 32-row block R. When every active row's bit blocks fall in one
+// range [c0, c0 + K) of at most kTileMaxK blocks, the rows form the A tile
+// (32 rows x K words, each word one 32-column mask); A is also the adjacency
+// of R, so the neighbours V of R are the set bits of the OR of A's rows. For
+// each group of 8 neighbours the warp gathers their masks on the same range
+// (the B tile) and one m16n8k256 b1 AND+POPC MMA per 16 rows per 8 words
+// gives D[r][j] = |N+(u_r) & N+(v_j)|; the count adds D[r][j] where A[r] has
+// v_j. Each neighbour's row is read once per row block instead of once per
+// edge. Row blocks that do not fit fall back to the bitmap sweep in place.
+
+constexpr int kTileStride = kTileMaxK + 4;      // padded: fragment loads hit 32 distinct banks
+constexpr int kTileMaxV = kTileMaxK * 32;
+constexpr int kTileWarps = 4;
+struct TileSmem {
+  uint32_t a[32 * kTileStride];                 // also the fallback hash table (4 KiB used)
+  uint32_t b[8 * kTileStride];
+  uint32_t vmask[kTileMaxK];
+  uint16_t vlist[kTileMaxV];
+};
+
+__device__ __forceinline__ void mma_b1(int (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                       uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k256.row.col.s32.b1.b1.s32.and.popc "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Per-row bitmap sweep of the active rows of a row block (the fallback).
+__device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl, unsigned long long* per_graph) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t acc = 0;
+  for (uint32_t r = 0; r < 32; ++r) {
+    const uint32_t u = rb * 32 + r;
+    if (u >= g.n) break;
+    const uint64_t a = g.rp[u], b = g.rp[u + 1];
+    const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
+    if (re - rs < 2 || nb > kWarpMaxBlocks) continue;
+    const int logb = table_logb(nb);
+    __syncwarp();
+    table_clear(tbl, logb, lane, 32);
+    __syncwarp();
+    table_insert(tbl, logb, g.bent, bs, be, lane, 32);
+    __syncwarp();
+    const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
+    const uint64_t racc =
+        sweep<true>(g, rs, re, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+    if (per_graph) {
+      const uint64_t s = warp_sum(racc);
+      if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
+    }
+    acc += racc;
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, const uint8_t* __restrict__ variant_of,
+                                                               uint32_t nrb, DeviceStats* stats,
+                                                               unsigned long long* per_graph,
+                                                               unsigned long long* block_ns) {
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  TileSmem& sm = reinterpret_cast<TileSmem*>(tile_raw)[threadIdx.x >> 5];
+  const uint32_t lane = threadIdx.x & 31, grp = lane >> 2, tig = lane & 3;
+  uint64_t acc = 0;
+  for (;;) {
+    uint32_t t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurVariant0 + TRIBIT_VARIANT_MMA], kGrab);
+    t0 = __shfl_sync(kFull, t0, 0);
+    if (t0 >= nrb) break;
+    const uint32_t t1 = min(t0 + kGrab, nrb);
+    for (uint32_t t = t0; t < t1; ++t) {
+      const uint32_t rb = nrb - 1 - t;
+      if (variant_of[rb] != TRIBIT_VARIANT_MMA) continue;
+      const unsigned long long t_start = (block_ns && lane == 0) ? cycles() : 0ull;
+      // Row of this lane: activity and block range.
+      const uint32_t u = rb * 32 + lane;
+      uint32_t bs = 0, be = 0, lo = 0xFFFFFFFFu, hi = 0;
+      bool active = false;
+      if (u < g.n) {
+        const uint64_t a = g.rp[u], b = g.rp[u + 1];
+        bs = rp_blk(a);
+        be = rp_blk(b);
+        active = rp_row(b) - rp_row(a) >= 2 && be - bs <= kWarpMaxBlocks;
+        if (active) {
+          lo = (uint32_t)(g.bent[bs] >> 32);
+          hi = (uint32_t)(g.bent[be - 1] >> 32);
+        }
+      }
+      const uint32_t amask = __ballot_sync(kFull, active);
+      if (!amask) continue;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+      }
+      const uint32_t K = hi - lo + 1;
+      uint64_t racc = 0;
+      if (K > (uint32_t)kTileMaxK) {
+        racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), per_graph);
+      } else {
+        const uint32_t KP = (K + 7) & ~7u;  // words, whole 256-bit k-steps
+        for (uint32_t i = lane; i < 32 * kTileStride; i += 32) sm.a[i] = 0u;
+        __syncwarp();
+        // A rows: each active row writes its own masks (distinct words).
+        for (uint32_t r = 0; r < 32; ++r) {
+          if (!((amask >> r) & 1u)) continue;
+          const uint32_t rbs = __shfl_sync(kFull, bs, r), rbe = __shfl_sync(kFull, be, r);
+          for (uint32_t k = rbs + lane; k < rbe; k += 32) {
+            const uint64_t e = g.bent[k];
+            sm.a[r * kTileStride + ((uint32_t)(e >> 32) - lo)] = (uint32_t)e;
+          }
+        }
+        __syncwarp();
+        // Neighbour set V: OR of the A rows, listed in column order.
+        uint32_t nv_total = 0;
+        for (uint32_t w0 = 0; w0 < KP; w0 += 32) {
+          const uint32_t w = w0 + lane;
+          uint32_t m = 0;
+          if (w < K)
+            for (uint32_t r = 0; r < 32; ++r) m |= sm.a[r * kTileStride + w];
+          const uint32_t c = __popc(m);
+          const uint32_t incl = warp_inclusive_sum(c);
+          uint32_t pos = nv_total + incl - c;
+          for (uint32_t bits = m; bits; bits &= bits - 1) sm.vlist[pos++] = (uint16_t)(w * 32 + __ffs(bits) - 1);
+          nv_total += __shfl_sync(kFull, incl, 31);
+        }
+        __syncwarp();
+        int rowsum[4] = {0, 0, 0, 0};  // rows grp, grp + 8, 16 + grp, 24 + grp
+        for (uint32_t j0 = 0; j0 < nv_total; j0 += 8) {
+          for (uint32_t i = lane; i < 8 * kTileStride; i += 32) sm.b[i] = 0u;
+          __syncwarp();
+          // B tile: the 8 neighbours' masks on [lo, lo + K).
+          for (uint32_t jj = 0; jj < 8 && j0 + jj < nv_total; ++jj) {
+            const uint32_t v = lo * 32 + sm.vlist[j0 + jj];
+            const uint64_t va = g.rp[v], vb = g.rp[v + 1];
+            const uint32_t vbs = rp_blk(va), vn = min(rp_blk(vb) - vbs, K);
+            for (uint32_t k = lane; k < vn; k += 32) {
+              const uint64_t e = g.bent[vbs + k];
+              const uint32_t blk = (uint32_t)(e >> 32);
+              if (blk <= hi) sm.b[jj * kTileStride + (blk - lo)] = (uint32_t)e;
+            }
+          }
+          __syncwarp();
+          int c0[4] = {0, 0, 0, 0}, c1[4] = {0, 0, 0, 0};
+          for (uint32_t ks = 0; ks < KP; ks += 8) {
+            const uint32_t* a0p = sm.a + grp * kTileStride + ks + tig;
+            const uint32_t* bp = sm.b + grp * kTileStride + ks + tig;
+            const uint32_t b0 = bp[0], b1 = bp[4];
+            mma_b1(c0, a0p[0], a0p[8 * kTileStride], a0p[4], a0p[8 * kTileStride + 4], b0, b1);
+            mma_b1(c1, a0p[16 * kTileStride], a0p[24 * kTileStride], a0p[16 * kTileStride + 4],
+                   a0p[24 * kTileStride + 4], b0, b1);
+          }
+          // D[row][col]: c[0] (grp, 2t), c[1] (grp, 2t+1), c[2] (grp+8, 2t), c[3] (grp+8, 2t+1).
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t col = 2 * tig + (q & 1);
+            if (j0 + col >= nv_total) continue;
+            const uint32_t vo = sm.vlist[j0 + col];
+            const uint32_t ra = grp + ((q >> 1) ? 8 : 0), rbb = ra + 16;
+            if ((sm.a[ra * kTileStride + (vo >> 5)] >> (vo & 31)) & 1u) rowsum[q >> 1] += c0[q];
+            if ((sm.a[rbb * kTileStride + (vo >> 5)] >> (vo & 31)) & 1u) rowsum[2 + (q >> 1)] += c1[q];
+          }
+          __syncwarp();
+        }
+        // Reduce the four lanes of each row group; lane tig == 0 owns the rows.
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          rowsum[q] += __shfl_xor_sync(kFull, rowsum[q], 1);
+          rowsum[q] += __shfl_xor_sync(kFull, rowsum[q], 2);
+        }
+        if (tig == 0) {
+          const uint32_t rows[4] = {grp, grp + 8, 16 + grp, 24 + grp};
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            racc += (uint64_t)rowsum[q];
+            if (per_graph && rowsum[q]) atomicAdd(&per_graph[g.graph_of_rank[rb * 32 + rows[q]]],
+                                                  (unsigned long long)rowsum[q]);
+          }
+        }
+        __syncwarp();
+      }
+      if (block_ns) {
+        __syncwarp();
+        if (lane == 0) atomicAdd(&block_ns[rb], cycles() - t_start);
+      }
+      acc += racc;
+    }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+}
+
+// ---- CTA-per-row pass for rows deferred by the warp kernels ---------------
 
 __device__ __forceinline__ uint64_t block_sum_u64(uint64_t v) {
   __shared__ unsigned long long part[kCtaThreads / 32];
@@ -204,10 +501,11 @@ __device__ __forceinline__ uint64_t block_sum_u64(uint64_t v) {
 
 __global__ void __launch_bounds__(kCtaThreads) k_rows_cta(GraphView g, const uint32_t* __restrict__ rows,
                                                            DeviceStats* stats, uint32_t* __restrict__ ovf_global,
-                                                           unsigned long long* per_graph) {
+                                                           unsigned long long* per_graph,
+                                                           unsigned long long* block_ns) {
   extern __shared__ __align__(16) uint64_t tbl[];
   __shared__ uint32_t s_t;
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t len = stats->overflow[kOvfCta];
   uint64_t acc = 0;
   for (;;) {
@@ -218,37 +516,32 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_cta(GraphView g, const uin
     if (t >= len) break;
     const uint32_t u = rows[t];
     const uint64_t a = g.rp[u], b = g.rp[u + 1];
-    const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nbu = be - bs;
-    if (nbu > kCtaMaxBlocks) {
+    const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
+    if (nb > kCtaMaxBlocks) {
       if (threadIdx.x == 0) push_row(stats, kOvfGlobal, ovf_global, u);
       continue;
     }
-    const int logsz = max(5, log2_ceil(2 * nbu));
-    table_clear(tbl, logsz, threadIdx.x, blockDim.x);
+    const unsigned long long t_start = block_ns ? cycles() : 0ull;
+    const int logb = table_logb(nb);
+    table_clear(tbl, logb, threadIdx.x, blockDim.x);
     __syncthreads();
-    table_insert(tbl, logsz, g.bent, bs, be, threadIdx.x, blockDim.x);
+    table_insert(tbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
     __syncthreads();
-    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32), bmax = (uint32_t)(g.bent[be - 1] >> 32);
-    uint64_t racc = sweep<true>(g, rs, re, w, nw, [&](uint32_t k, uint32_t) -> uint32_t {
-      uint64_t e = g.bent[k];
-      uint32_t blk = (uint32_t)(e >> 32);
-      if (blk < bmin || blk > bmax) return 0u;
-      return (uint32_t)__popc((uint32_t)e & table_find(tbl, logsz, blk));
-    });
-    if (per_graph) {
-      uint64_t s = block_sum_u64(racc);
-      if (threadIdx.x == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
-    } else {
-      __syncthreads();  // the table is rebuilt for the next row
+    const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
+    const uint64_t racc =
+        sweep<true>(g, rs, re, w, nw, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+    const uint64_t s = block_sum_u64(racc);  // also the barrier before the table is rebuilt
+    if (threadIdx.x == 0) {
+      if (per_graph && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
+      if (block_ns) atomicAdd(&block_ns[u >> 5], cycles() - t_start);
     }
     acc += racc;
   }
-  (void)lane;
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
-// ---- global-memory pass: any row size, merge by binary search in global ---
+// ---- global-memory pass: any row size, binary search in global memory -----
 
 __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const uint32_t* __restrict__ rows,
                                                               DeviceStats* stats, unsigned long long* per_graph) {
@@ -265,12 +558,12 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
     const uint32_t u = rows[t];
     const uint32_t rs = rp_row(g.rp[u]), re = rp_row(g.rp[u + 1]);
     const uint32_t last = g.col[re - 1];
-    uint64_t racc = sweep<false>(g, rs, re, w, nw, [&](uint32_t k, uint32_t c) -> uint32_t {
-      uint32_t x = g.col[k];
+    const uint64_t racc = sweep<false>(g, rs, re, w, nw, [&](uint32_t k, uint32_t c) -> uint32_t {
+      const uint32_t x = g.col[k];
       if (x > last) return 0u;
       uint32_t lo = c + 1, hi = re;
       while (lo < hi) {
-        uint32_t mid = lo + ((hi - lo) >> 1);
+        const uint32_t mid = lo + ((hi - lo) >> 1);
         if (g.col[mid] < x)
           lo = mid + 1;
         else
@@ -278,17 +571,15 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
       }
       return (lo < re && g.col[lo] == x) ? 1u : 0u;
     });
-    if (per_graph) {
-      uint64_t s = block_sum_u64(racc);
-      if (threadIdx.x == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
-    }
+    const uint64_t s = block_sum_u64(racc);
+    if (threadIdx.x == 0 && per_graph && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
     acc += racc;
   }
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
-// ---- schedule ------------------------------------------------------------
+// ---- schedule ----------------------------------------------------------------
 
 // Row-block features (one warp per row block) and the plain dispatcher's
 // choice. Features are log-scaled so the learned dispatcher sees O(1) inputs.
@@ -298,35 +589,44 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
-    uint32_t u = rb * 32 + lane;
-    uint32_t d = 0, nbu = 0;
+    const uint32_t u = rb * 32 + lane;
+    uint32_t d = 0, nbu = 0, lo = 0xFFFFFFFFu, hi = 0;
     if (u < g.n) {
-      uint64_t a = g.rp[u], b = g.rp[u + 1];
+      const uint64_t a = g.rp[u], b = g.rp[u + 1];
       d = rp_row(b) - rp_row(a);
       nbu = rp_blk(b) - rp_blk(a);
+      if (d >= 2 && nbu <= kWarpMaxBlocks) {
+        lo = (uint32_t)(g.bent[rp_blk(a)] >> 32);
+        hi = (uint32_t)(g.bent[rp_blk(b) - 1] >> 32);
+      }
     }
-    uint32_t active = d >= 2 ? 1u : 0u;
-    float fd = (float)d;
-    float rows = (float)warp_sum(active);
-    float nnz = (float)warp_sum(d);
-    float nb = (float)warp_sum(nbu);
-    float sq = warp_sum(fd * fd);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+      hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    const float span = hi >= lo ? (float)(hi - lo + 1) : 0.f;  // column blocks the tile would cover
+    const float fd = (float)d;
+    const float rows = (float)warp_sum(d >= 2 ? 1u : 0u);
+    const float nnz = (float)warp_sum(d);
+    const float nb = (float)warp_sum(nbu);
+    const float sq = warp_sum(fd * fd);
     uint32_t dmax = d;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(kFull, dmax, o));
-    // Neighbour-side work: bit blocks and ids the sweeps will read.
+    // Neighbour-side work: the bit blocks and ids the sweeps will read.
     float wb = 0.f, wm = 0.f, vmax = 0.f, top = 0.f;
     if (full) {
       for (uint32_t r = 0; r < 32; ++r) {
-        uint32_t ur = rb * 32 + r;
+        const uint32_t ur = rb * 32 + r;
         if (ur >= g.n) break;
-        uint64_t a = g.rp[ur], b = g.rp[ur + 1];
-        uint32_t rs = rp_row(a), re = rp_row(b);
+        const uint64_t a = g.rp[ur], b = g.rp[ur + 1];
+        const uint32_t rs = rp_row(a), re = rp_row(b);
         if (re - rs < 2) continue;
         for (uint32_t k = rs + lane; k < re; k += 32) {
-          uint32_t v = g.col[k];
-          uint64_t va = g.rp[v], vb = g.rp[v + 1];
-          float dv = (float)(rp_row(vb) - rp_row(va));
+          const uint32_t v = g.col[k];
+          const uint64_t va = g.rp[v], vb = g.rp[v + 1];
+          const float dv = (float)(rp_row(vb) - rp_row(va));
           wb += (float)(rp_blk(vb) - rp_blk(va));
           wm += dv;
           vmax = fmaxf(vmax, dv);
@@ -341,7 +641,7 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
     }
     if (lane == 0) {
       float* f = feat + (size_t)rb * kNumFeatures;
-      float mean = rows > 0 ? nnz / fmaxf(rows, 1.f) : 0.f;
+      const float mean = rows > 0 ? nnz / fmaxf(rows, 1.f) : 0.f;
       f[0] = rows / 32.f;
       f[1] = log2f(1.f + nnz);
       f[2] = log2f(1.f + nb);
@@ -355,127 +655,189 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
       f[10] = log2f(1.f + vmax);
       f[11] = nnz > 0 ? top / nnz : 0.f;
       f[12] = (float)rb * 32.f / fmaxf((float)g.n, 1.f);
-      f[13] = log2f(1.f + (float)g.n) / 32.f;
+      f[13] = log2f(1.f + span);
       f[14] = nnz > 0 ? log2f(1.f + wb / nnz) : 0.f;
       f[15] = log2f(1.f + sq);
-      uint8_t var;
-      if (mode == TRIBIT_DISPATCH_MERGE)
-        var = TRIBIT_VARIANT_MERGE;
-      else if (mode == TRIBIT_DISPATCH_BITMAP || mode == TRIBIT_DISPATCH_MMA)
-        var = TRIBIT_VARIANT_BITMAP;
-      else
-        var = TRIBIT_VARIANT_BITMAP;
-      if (rows == 0.f) var = TRIBIT_VARIANT_MERGE;  // nothing to count; cheapest skip
+      // Plain dispatcher: fixed thresholds. Bit tiles where the block's rows
+      // share one narrow column range and have enough edges to share
+      // neighbours; the bitmap sweep everywhere else.
+      uint8_t var = TRIBIT_VARIANT_BITMAP;
+      if (span > 0.f && span <= (float)kTileMaxK && nnz >= 64.f) var = TRIBIT_VARIANT_MMA;
+      if (mode == TRIBIT_DISPATCH_BITMAP) var = TRIBIT_VARIANT_BITMAP;
+      if (mode == TRIBIT_DISPATCH_MERGE) var = TRIBIT_VARIANT_MERGE;
+      if (mode == TRIBIT_DISPATCH_MMA) var = TRIBIT_VARIANT_MMA;
       variant_of[rb] = var;
     }
   }
 }
 
-// Packs (is MMA << 32) | is BITMAP for a scan; merge positions follow.
-__global__ void k_variant_flags(const uint8_t* __restrict__ variant_of, uint32_t nrb, uint64_t* __restrict__ flags) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nrb) return;
-  uint64_t f = 0;
-  if (i < nrb) {
-    uint8_t v = variant_of[i];
-    f = (v == TRIBIT_VARIANT_MMA ? (1ull << 32) : 0ull) | (v == TRIBIT_VARIANT_BITMAP ? 1ull : 0ull);
-  }
-  flags[i] = f;
+// Pieces of row u; rows wider than a warp's table are counted whole in the
+// heavy phase instead and get none.
+__device__ __forceinline__ uint32_t row_pieces(const GraphView& g, uint32_t u) {
+  if (u >= g.n) return 0u;
+  const uint64_t a = g.rp[u], b = g.rp[u + 1];
+  const uint32_t d = rp_row(b) - rp_row(a);
+  if (d < 2 || rp_blk(b) - rp_blk(a) > kWarpMaxBlocks) return 0u;
+  return (d + kPieceNeighbours - 1) / kPieceNeighbours;
 }
 
-__global__ void k_variant_lists(const uint8_t* __restrict__ variant_of, uint32_t nrb, const uint64_t* __restrict__ pos,
-                                uint32_t* l_mma, uint32_t* l_bitmap, uint32_t* l_merge, uint32_t* list_len) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nrb) {
-    uint64_t p = pos[i];
-    uint32_t pm = (uint32_t)(p >> 32), pb = (uint32_t)p;
-    uint8_t v = variant_of[i];
-    if (v == TRIBIT_VARIANT_MMA)
-      l_mma[pm] = i;
-    else if (v == TRIBIT_VARIANT_BITMAP)
-      l_bitmap[pb] = i;
-    else
-      l_merge[i - pm - pb] = i;
+__global__ void k_heavy_flags(GraphView g, uint32_t* __restrict__ flags) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u > g.n) return;
+  uint32_t f = 0;
+  if (u < g.n) {
+    const uint64_t a = g.rp[u], b = g.rp[u + 1];
+    f = (rp_row(b) - rp_row(a) >= 2 && rp_blk(b) - rp_blk(a) > kWarpMaxBlocks) ? 1u : 0u;
   }
-  if (i == nrb) {
-    uint64_t p = pos[nrb];
-    list_len[TRIBIT_VARIANT_MMA] = (uint32_t)(p >> 32);
-    list_len[TRIBIT_VARIANT_BITMAP] = (uint32_t)p;
-    list_len[TRIBIT_VARIANT_MERGE] = nrb - (uint32_t)(p >> 32) - (uint32_t)p;
+  flags[u] = f;
+}
+
+__global__ void k_heavy_scatter(GraphView g, const uint32_t* __restrict__ pos, uint32_t* __restrict__ heavy,
+                                uint32_t* __restrict__ piece_off) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < g.n && pos[u + 1] != pos[u]) heavy[pos[u]] = u;
+  if (u == g.n) piece_off[TRIBIT_NUM_VARIANTS + 1] = pos[g.n];
+}
+
+// Pieces of each row block (one warp per row block).
+__global__ void k_block_pieces(GraphView g, uint32_t nrb, uint32_t* __restrict__ cnt) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
+    const uint32_t s = warp_sum(row_pieces(g, rb * 32 + lane));
+    if (lane == 0) cnt[rb] = s;
+  }
+}
+
+__global__ void k_piece_flags(const uint8_t* __restrict__ variant_of, const uint32_t* __restrict__ cnt, uint32_t nrb,
+                              int v, uint32_t* __restrict__ flags, uint32_t* __restrict__ list_len) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nrb) flags[i] = variant_of[i] == v ? cnt[i] : 0u;
+  if (i == nrb) flags[i] = 0u;
+  // row blocks per variant, for reporting
+  if (i < nrb && variant_of[i] == v && cnt[i]) atomicAdd(&list_len[v], 1u);
+}
+
+__global__ void k_piece_segment(const uint32_t* __restrict__ off, uint32_t nrb, int v, uint32_t* piece_off) {
+  if (v == 0) piece_off[0] = 0u;
+  piece_off[v + 1] = piece_off[v] + off[nrb];
+}
+
+__global__ void k_piece_scatter(GraphView g, uint32_t nrb, const uint8_t* __restrict__ variant_of, int v,
+                                const uint32_t* __restrict__ off, const uint32_t* __restrict__ piece_off,
+                                uint64_t* __restrict__ pieces) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t seg = piece_off[v];
+  for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
+    if (variant_of[rb] != v) continue;
+    const uint32_t u = rb * 32 + lane;
+    const uint32_t np = row_pieces(g, u);
+    const uint32_t incl = warp_inclusive_sum(np);
+    const uint32_t base = seg + off[rb] + incl - np;
+    for (uint32_t k = 0; k < np; ++k) pieces[base + k] = ((uint64_t)u << 32) | (k * kPieceNeighbours);
   }
 }
 
 }  // namespace
 
-Schedule take_schedule(Arena& ar, uint64_t n) {
+Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E) {
   Schedule s;
-  uint32_t nrb = (uint32_t)ceil_div<uint64_t>(n, 32);
+  const uint32_t nrb = (uint32_t)ceil_div<uint64_t>(n, 32);
   s.num_row_blocks = nrb;
   s.variant_of = ar.take<uint8_t>(nrb + 1);
-  for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) s.list[v] = ar.take<uint32_t>(nrb + 1);
+  s.piece_cap = n + E / kPieceNeighbours + 64;
+  s.pieces = ar.take<uint64_t>(s.piece_cap);
+  s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 2);
+  s.heavy = ar.take<uint32_t>(n + 1);
+  s.row_flags = ar.take<uint32_t>(n + 1);
+  s.row_scan_tmp = take_scan_temp<uint32_t>(ar, n + 1);
   s.list_len = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS);
+  s.block_pieces = ar.take<uint32_t>(nrb + 1);
+  s.flags = ar.take<uint32_t>(nrb + 1);
+  s.scan_tmp = take_scan_temp<uint32_t>(ar, nrb + 1);
   s.overflow_cap = (uint32_t)(n + 1);
   s.overflow = ar.take<uint32_t>(2 * (n + 1));
   s.features = ar.take<float>((uint64_t)nrb * kNumFeatures + 1);
-  s.flags = reinterpret_cast<uint32_t*>(ar.take<uint64_t>(nrb + 1));
-  s.scan_tmp = reinterpret_cast<uint32_t*>(take_scan_temp<uint64_t>(ar, nrb + 1));
   return s;
 }
 
-void build_schedule(const GraphView& g, Schedule& s, int mode, const void* /*mlp*/, cudaStream_t st) {
+void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
   const uint32_t nrb = s.num_row_blocks;
-  if (nrb > 0) {
-    unsigned blocks = (unsigned)std::min<uint64_t>(ceil_div<uint64_t>(nrb, 8), 148ull * 16);
-    k_features<<<blocks, 256, 0, st>>>(g, nrb, mode, s.features, s.variant_of, 0);
+  const unsigned wblocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(nrb, 8), 148ull * 16));
+  const unsigned fblocks = (unsigned)ceil_div<uint64_t>(nrb + 1, 256);
+  TB_CUDA(cudaMemsetAsync(s.list_len, 0, TRIBIT_NUM_VARIANTS * sizeof(uint32_t), st));
+  if (nrb) {
+    k_block_pieces<<<wblocks, 256, 0, st>>>(g, nrb, s.block_pieces);
     TB_LAUNCH_CHECK();
   }
-  uint64_t* flags = reinterpret_cast<uint64_t*>(s.flags);
-  k_variant_flags<<<(unsigned)ceil_div<uint64_t>(nrb + 1, 256), 256, 0, st>>>(s.variant_of, nrb, flags);
+  for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) {
+    k_piece_flags<<<fblocks, 256, 0, st>>>(s.variant_of, s.block_pieces, nrb, v, s.flags, s.list_len);
+    TB_LAUNCH_CHECK();
+    device_scan<uint32_t, OpSum>(s.flags, s.flags, nrb + 1, true, OpSum{}, 0u, s.scan_tmp, st);
+    k_piece_segment<<<1, 1, 0, st>>>(s.flags, nrb, v, s.piece_off);
+    TB_LAUNCH_CHECK();
+    if (nrb) {
+      k_piece_scatter<<<wblocks, 256, 0, st>>>(g, nrb, s.variant_of, v, s.flags, s.piece_off, s.pieces);
+      TB_LAUNCH_CHECK();
+    }
+  }
+  const unsigned rblocks = (unsigned)ceil_div<uint64_t>((uint64_t)g.n + 1, 256);
+  k_heavy_flags<<<rblocks, 256, 0, st>>>(g, s.row_flags);
   TB_LAUNCH_CHECK();
-  device_scan<uint64_t, OpSum>(flags, flags, nrb + 1, true, OpSum{}, 0ull, reinterpret_cast<uint64_t*>(s.scan_tmp), st);
-  k_variant_lists<<<(unsigned)ceil_div<uint64_t>(nrb + 1, 256), 256, 0, st>>>(
-      s.variant_of, nrb, flags, s.list[TRIBIT_VARIANT_MMA], s.list[TRIBIT_VARIANT_BITMAP], s.list[TRIBIT_VARIANT_MERGE],
-      s.list_len);
+  device_scan<uint32_t, OpSum>(s.row_flags, s.row_flags, (uint64_t)g.n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
+  k_heavy_scatter<<<rblocks, 256, 0, st>>>(g, s.row_flags, s.heavy, s.piece_off);
   TB_LAUNCH_CHECK();
 }
 
+void compute_features(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st) {
+  const uint32_t nrb = s.num_row_blocks;
+  if (nrb == 0) return;
+  const unsigned blocks = (unsigned)std::min<uint64_t>(ceil_div<uint64_t>(nrb, 8), 148ull * 16);
+  k_features<<<blocks, 256, 0, st>>>(g, nrb, mode, s.features, s.variant_of, full_features ? 1 : 0);
+  TB_LAUNCH_CHECK();
+}
+
+void build_schedule(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st) {
+  compute_features(g, s, mode, full_features, st);
+  build_pieces(g, s, st);
+}
+
 LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stats, unsigned long long* per_graph,
-                      const CountConfig& cfg, cudaStream_t st) {
+                        const CountConfig& cfg, cudaStream_t st) {
   static bool attr_done = false;
   if (!attr_done) {
     TB_CUDA(cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(uint64_t) << kCtaLogSlots)));
+    TB_CUDA(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kTileWarps * sizeof(TileSmem))));
     attr_done = true;
   }
   const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
   const int per_sm = cfg.ctas_per_sm > 0 ? cfg.ctas_per_sm : 6;
   const unsigned warp_grid = (unsigned)(sms * per_sm);
   LaunchInfo info;
-  uint64_t& ctas = info.ctas;
   TB_CUDA(cudaMemsetAsync(stats->cursor, 0, sizeof(stats->cursor) + sizeof(stats->overflow), st));
   TB_CUDA(cudaMemsetAsync(&stats->triangles, 0, sizeof(stats->triangles), st));
   uint32_t* ovf_cta = s.overflow;
   uint32_t* ovf_global = s.overflow + s.overflow_cap;
-  // The MMA list is counted by the bitmap kernel until the tile kernel lands.
-  k_rows_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-      g, s.list[TRIBIT_VARIANT_BITMAP], s.list_len, stats, ovf_cta, per_graph);
+  k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
+      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy);
   TB_LAUNCH_CHECK();
-  ctas += warp_grid;
-  k_rows_warp<TRIBIT_VARIANT_MMA><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.list[TRIBIT_VARIANT_MMA], s.list_len,
-                                                                           stats, ovf_cta, per_graph);
+  k_tiles_mma<<<(unsigned)(sms * 3), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
+      g, s.variant_of, s.num_row_blocks, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
-  ctas += warp_grid;
-  k_rows_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-      g, s.list[TRIBIT_VARIANT_MERGE], s.list_len, stats, ovf_cta, per_graph);
+  k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
+                                                                               per_graph, cfg.block_ns, nullptr);
   TB_LAUNCH_CHECK();
-  ctas += warp_grid;
   k_rows_cta<<<(unsigned)sms, kCtaThreads, sizeof(uint64_t) << kCtaLogSlots, st>>>(g, ovf_cta, stats, ovf_global,
-                                                                                   per_graph);
+                                                                                   per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
-  ctas += sms;
   k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
   TB_LAUNCH_CHECK();
-  ctas += sms;
+  info.ctas = 2ull * warp_grid + 5ull * sms;
   info.kernels = 5;
   return info;
 }

@@ -5,6 +5,13 @@
 // reference accumulates as sum popc(U(u, blk) & L(v, blk)) in
 // compute_binary_popcount_mma_9 (tribit.cu:519-586), whose per-lane binary
 // searches and one-row-in-eight b1 MMA tiles it replaces.
+//
+// Work is scheduled in two levels. The dispatcher assigns every 32-row block
+// of the oriented graph one counting variant (row-block features -> plain
+// thresholds or the learned MLP). Each variant's rows are then cut into
+// pieces of at most kPieceNeighbours neighbours, so one heavy row is spread
+// over many warps; the variant kernels are persistent and pull pieces from a
+// device cursor.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -14,41 +21,57 @@
 
 namespace tb {
 
-// Per-32-row-block schedule: which variant counts each row block.
+constexpr int kNumFeatures = 16;
+constexpr uint32_t kPieceNeighbours = 64;
+
 struct Schedule {
   uint32_t num_row_blocks = 0;
-  uint8_t* variant_of = nullptr;                   // device, num_row_blocks
-  uint32_t* list[TRIBIT_NUM_VARIANTS] = {};        // device, row blocks of each variant
-  uint32_t* list_len = nullptr;                    // device, TRIBIT_NUM_VARIANTS
-  uint32_t* overflow = nullptr;                    // device, rows deferred to wider paths
-  uint32_t overflow_cap = 0;
-  float* features = nullptr;                       // device, num_row_blocks x kNumFeatures
+  uint8_t* variant_of = nullptr;   // device, per row block
+  uint64_t* pieces = nullptr;      // device, (row << 32) | first neighbour, grouped by variant
+  uint64_t piece_cap = 0;
+  uint32_t* piece_off = nullptr;   // device, TRIBIT_NUM_VARIANTS + 1 segment starts, then the heavy-row count
+  uint32_t* heavy = nullptr;       // device, rows too wide for one warp, counted CTA-cooperatively first
+  uint32_t* row_flags = nullptr;   // device, n + 1 scratch for the heavy-row scan
+  uint32_t* row_scan_tmp = nullptr;
+  uint32_t* list_len = nullptr;    // device, row blocks per variant
+  uint32_t* block_pieces = nullptr;// device, pieces per row block
+  uint32_t* flags = nullptr;       // device, nrb + 1 scratch for the scans
   uint32_t* scan_tmp = nullptr;
-  uint32_t* flags = nullptr;
+  uint32_t* overflow = nullptr;    // device, rows deferred to the CTA / global passes
+  uint32_t overflow_cap = 0;
+  float* features = nullptr;       // device, nrb x kNumFeatures
+  const void* model = nullptr;     // device MLP parameters for learned dispatch
 };
-
-constexpr int kNumFeatures = 16;
 
 // Per-launch configuration chosen by the autotuner (or defaults).
 struct CountConfig {
-  int ctas_per_sm = 0;     // 0 = default
+  int ctas_per_sm = 0;  // 0 = default
   int num_sms = 148;
+  unsigned long long* block_ns = nullptr;  // optional: per-row-block SM cycles, summed over pieces
 };
 
-Schedule take_schedule(Arena& ar, uint64_t n);
+Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E);
 
-// Computes row-block features and the per-variant work lists.
-// mode: TRIBIT_DISPATCH_* ; mlp_weights: device weights for LEARNED (or null).
-void build_schedule(const GraphView& g, Schedule& s, int mode, const void* mlp, cudaStream_t st);
+// Computes row-block features, the per-block variant (mode: TRIBIT_DISPATCH_*),
+// and the per-variant piece lists. full_features adds the neighbour-side
+// features (one extra pass over the edges) the learned dispatcher needs.
+void build_schedule(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st);
+
+// Row-block features (full adds the neighbour-side ones) and the plain or
+// forced variant for every row block; build_schedule = this + build_pieces.
+void compute_features(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st);
+
+// Re-derives the piece lists after variant_of was rewritten (learned dispatch).
+void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st);
 
 struct LaunchInfo {
-  uint64_t ctas = 0;      // CTAs over all counting kernels
-  uint32_t kernels = 0;   // kernel launches
+  uint64_t ctas = 0;     // CTAs over all counting kernels
+  uint32_t kernels = 0;  // kernel launches
 };
 
 // Launches every counting kernel; the exact count lands in stats->triangles
 // (and per_graph[g] in batch mode).
 LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stats, unsigned long long* per_graph,
-                      const CountConfig& cfg, cudaStream_t st);
+                        const CountConfig& cfg, cudaStream_t st);
 
 }  // namespace tb

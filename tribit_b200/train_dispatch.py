@@ -1,0 +1,170 @@
+"""Trains the learned dispatcher from timings the counter records itself.
+
+For each training graph (generated here, with seeds disjoint from the
+benchmark's) the counter prepares the graph on the GPU, reads the 16
+features of every 32-row block (tribit_block_features), then counts the whole
+graph once per variant with every row block forced onto that variant,
+recording the SM cycles each row block took (tribit_block_times). The MLP
+(16 -> 64 -> 64 -> 3) is trained on the GPU by the library's own forward,
+backward and Adam kernels (tribit_model_train) to predict log2(1 + cycles) of
+each variant, and is evaluated on a held-out graph: total cycles of the
+plain dispatcher's choice, of the MLP's choice and of the per-block best
+(regret = chosen - best), plus the measured counting time under each
+dispatcher.
+
+  python -m tribit_b200.train_dispatch [--out tribit_b200/models/dispatch_mlp.bin] [--quick]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+import tribit_b200 as tb
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(HERE, "models", "dispatch_mlp.bin")
+
+
+def batch_union(num_graphs: int, seed: int):
+    """Disjoint union of small ER / Chung-Lu graphs (the batched workload's mix)."""
+    rng = np.random.default_rng(seed)
+    parts, base = [], 0
+    for g in range(num_graphs):
+        n = int(round(64 * 1024 ** rng.uniform()))
+        d = rng.uniform(8, 64)
+        if rng.uniform() < 0.5:
+            e = tb.gen_er(n, int(n * d / 2), seed=seed * 100003 + g)
+        else:
+            e = tb.gen_chung_lu(n, int(n * d / 2), float(rng.uniform(2.1, 2.8)), max(4.0, n / 8), seed=seed * 100003 + g)
+        hi = (e >> np.uint64(32)) + np.uint64(base)
+        lo = (e & np.uint64(0xFFFFFFFF)) + np.uint64(base)
+        parts.append((hi << np.uint64(32)) | lo)
+        base += n
+    return base, np.concatenate(parts)
+
+
+def training_graphs(quick: bool):
+    if quick:
+        return [("rmat18_s118", lambda: (1 << 18, tb.gen_rmat(18, 16, seed=118))),
+                ("planted_s103", lambda: (400_000, tb.gen_planted(4000, 100, 0.3, 2, seed=103))),
+                ("batch_s101", lambda: batch_union(64, 101))]
+    return [("rmat22_s122", lambda: (1 << 22, tb.gen_rmat(22, 16, seed=122))),
+            ("rmat21_s121", lambda: (1 << 21, tb.gen_rmat(21, 16, seed=121))),
+            ("planted_s103", lambda: (2_000_000, tb.gen_planted(20000, 100, 0.3, 2, seed=103))),
+            ("batch_s101", lambda: batch_union(512, 101))]
+
+
+def holdout_graph(quick: bool):
+    if quick:
+        return "rmat17_s7", (1 << 17, tb.gen_rmat(17, 16, seed=7))
+    return "rmat22_s7", (1 << 22, tb.gen_rmat(22, 16, seed=7))
+
+
+def collect(n, e, repeats: int = 2):
+    import torch
+    d = torch.from_numpy(e.view(np.int64)).cuda()
+    with tb.Counter(dispatch="plain") as c:
+        c.prepare_device(d.data_ptr(), d.numel(), n)
+        x = c.block_features()
+        times, tri = [], set()
+        for v in tb.VARIANTS:
+            runs = []
+            for _ in range(repeats):
+                t, count = c.block_times(v)
+                runs.append(t)
+                tri.add(count)
+            times.append(np.minimum.reduce(runs))
+        assert len(tri) == 1, "variants disagree on the count"
+    t = np.stack(times, 1)
+    keep = t.max(1) > 0
+    return x[keep], t[keep], x, t
+
+
+def plain_choice(x):
+    """The plain dispatcher's rule, restated on the features (for the regret table)."""
+    nnz = np.exp2(x[:, 1]) - 1
+    span = np.exp2(x[:, 13]) - 1
+    choice = np.full(x.shape[0], tb.VARIANTS.index("bitmap"))
+    mma = (span > 0.5) & (span <= 64.5) & (nnz >= 63.5)
+    choice[mma] = tb.VARIANTS.index("mma")
+    return choice
+
+
+def timed_count(n, e, dispatch, model, steps=5):
+    import torch
+    d = torch.from_numpy(e.view(np.int64)).cuda()
+    with tb.Counter(dispatch=dispatch) as c:
+        if dispatch == "learned":
+            c.load_model(model)
+        s = torch.cuda.Stream()
+        c.set_stream(s.cuda_stream)
+        c.prepare_device(d.data_ptr(), d.numel(), n)
+        ms = []
+        with torch.cuda.stream(s):
+            c.launch_count()
+            for _ in range(steps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s)
+                c.launch_count()
+                b.record(s)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+        r = c.read_count()
+    return float(np.median(ms)), r.triangles, dict(zip(tb.VARIANTS, r.row_blocks_by_variant))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    args = ap.parse_args()
+
+    xs, ys = [], []
+    for name, make in training_graphs(args.quick):
+        t0 = time.time()
+        n, e = make()
+        x, t, _, _ = collect(n, e)
+        xs.append(x)
+        ys.append(np.log2(1.0 + t))
+        print(json.dumps({"graph": name, "row_blocks": int(x.shape[0]), "seconds": round(time.time() - t0, 1),
+                          "cycles_per_variant": dict(zip(tb.VARIANTS, map(float, t.sum(0))))}), flush=True)
+    X = np.concatenate(xs).astype(np.float32)
+    Y = np.concatenate(ys).astype(np.float32)
+    norm = np.concatenate([X.mean(0), X.std(0) + 1e-3, Y.mean(0), Y.std(0) + 1e-3]).astype(np.float32)
+
+    hname, (hn, he) = holdout_graph(args.quick)
+    hx, ht, _, _ = collect(hn, he)
+    with tb.Counter() as c:
+        c.model_init(norm, seed=args.seed)
+        loss = c.model_train(X, Y, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed)
+        os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+        c.save_model(args.out)
+        pred = c.model_predict(hx)
+    learned = pred.argmin(1)
+    plain = plain_choice(hx)
+    rows = np.arange(ht.shape[0])
+    best = ht.min(1).sum()
+    report = {
+        "train_rows": int(X.shape[0]), "final_loss": loss, "holdout": hname,
+        "holdout_cycles": {"best": float(best), "plain": float(ht[rows, plain].sum()),
+                           "learned": float(ht[rows, learned].sum()),
+                           **{f"all_{v}": float(ht[:, i].sum()) for i, v in enumerate(tb.VARIANTS)}},
+        "learned_picks": dict(zip(tb.VARIANTS, np.bincount(learned, minlength=3).tolist())),
+        "plain_picks": dict(zip(tb.VARIANTS, np.bincount(plain, minlength=3).tolist())),
+    }
+    p_ms, p_tri, _ = timed_count(hn, he, "plain", args.out)
+    l_ms, l_tri, _ = timed_count(hn, he, "learned", args.out)
+    assert p_tri == l_tri
+    report["holdout_count_ms"] = {"plain": p_ms, "learned": l_ms}
+    print(json.dumps(report), flush=True)
+
+
+if __name__ == "__main__":
+    main()
