@@ -194,9 +194,11 @@ tribit_status tribit_model_train(tribit_context* ctx, const float* x, const floa
 tribit_status tribit_block_features(tribit_context* ctx, float* out, uint64_t cap, uint64_t* num_row_blocks);
 /* Counts with every row block on `variant` (TRIBIT_VARIANT_*) and records the
  * SM cycles each row block's pieces took (cycles_out[num_row_blocks]);
- * *triangles receives the count, which equals the normal one. */
+ * *triangles receives the count, which equals the normal one, and
+ * *variant_ms the device time of the variant kernels (the rows too wide for
+ * a warp, which every variant shares, run before it and are excluded). */
 tribit_status tribit_block_times(tribit_context* ctx, int variant, float* cycles_out, uint64_t cap,
-                                 uint64_t* triangles);
+                                 uint64_t* triangles, float* variant_ms);
 
 /* ---- synthetic graphs (host, seeded, thread-count independent) ---------- */
 tribit_status tribit_gen_rmat(int scale, uint64_t edge_factor, double a, double b, double c, uint64_t seed,

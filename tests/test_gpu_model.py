@@ -98,8 +98,8 @@ def test_block_features_and_times():
         f = c.block_features()
         assert f.shape == ((n + 31) // 32, 16) and np.isfinite(f).all()
         for v in tb.VARIANTS:
-            t, tri = c.block_times(v)
-            assert tri == want
+            t, tri, ms = c.block_times(v)
+            assert tri == want and ms > 0
             assert t.shape[0] == f.shape[0] and (t >= 0).all() and t.sum() > 0
         c.launch_count()
         assert c.read_count().triangles == want

@@ -89,7 +89,8 @@ _decl("tribit_model_gradients", ctypes.c_int, _p, _p, _p, _u64, _p, ctypes.POINT
 _decl("tribit_model_train", ctypes.c_int, _p, _p, _p, _u64, _u32, _u32, ctypes.c_float, _u64,
       ctypes.POINTER(ctypes.c_float))
 _decl("tribit_block_features", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
-_decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POINTER(_u64))
+_decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POINTER(_u64),
+      ctypes.POINTER(ctypes.c_float))
 _decl("tribit_count_edges_noalloc", ctypes.c_int, _p, _u64, _u64, _p, _p)
 _decl("tribit_noalloc_scratch_bytes", _u64)
 _decl("tribit_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, _p)
@@ -231,9 +232,10 @@ class Counter:
         _check(lib.tribit_block_features(self._h, None, 0, ctypes.byref(nrb)), self._h)
         out = np.zeros(nrb.value, dtype=np.float32)
         tri = _u64()
+        ms = ctypes.c_float()
         _check(lib.tribit_block_times(self._h, VARIANTS.index(variant), out.ctypes.data, out.size,
-                                      ctypes.byref(tri)), self._h)
-        return out, tri.value
+                                      ctypes.byref(tri), ctypes.byref(ms)), self._h)
+        return out, tri.value, ms.value
 
     def count_edges(self, entries, num_nodes: int) -> Result:
         e = _entries(entries)

@@ -20,7 +20,6 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kWarpsPerCta = 8;
 constexpr int kWarpSlots = 512;                      // 8-byte words of shared memory per warp
 constexpr uint32_t kWarpMaxBlocks = kWarpSlots / 2;  // bitmap rows up to this many bit blocks
-constexpr uint32_t kWarpMaxList = kWarpSlots * 2;    // merge rows up to this many neighbours
 constexpr int kCtaThreads = 512;
 constexpr int kCtaLogSlots = 14;                     // 16384 slots = 128 KiB
 constexpr uint32_t kCtaMaxBlocks = (1u << kCtaLogSlots) / 2;
@@ -146,6 +145,91 @@ __device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint3
   return acc;
 }
 
+// Mask of block x in the sorted bit row r[lo, end), or 0.
+__device__ __forceinline__ uint32_t search_mask(const uint64_t* r, uint32_t lo, uint32_t end, uint32_t x) {
+  uint32_t hi = end;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((uint32_t)(r[mid] >> 32) < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < end) {
+    const uint64_t e = r[lo];
+    if ((uint32_t)(e >> 32) == x) return (uint32_t)e;
+  }
+  return 0u;
+}
+
+// Sorted-list intersection of bit rows (the merge variant). u's bit row is in
+// shared memory (urow, nbu entries, ascending block). For each neighbour v of
+// the chunk, the shorter of u's tail -- u's entries from v's block on, the
+// only ones that can meet N+(v) -- and v's bit row is walked, and every block
+// of it is binary-searched in the other list. Must be called by all 32 lanes.
+__device__ __forceinline__ uint64_t sweep_merge(const GraphView& g, const uint64_t* urow, uint32_t nbu, uint32_t cs,
+                                                uint32_t ce) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t acc = 0;
+  auto item = [&](uint32_t k, bool walk_u, uint32_t ob, uint32_t oe) -> uint32_t {
+    const uint64_t e = walk_u ? urow[k] : g.bent[k];
+    const uint32_t m = walk_u ? search_mask(g.bent, ob, oe, (uint32_t)(e >> 32))
+                              : search_mask(urow, ob, oe, (uint32_t)(e >> 32));
+    return (uint32_t)__popc((uint32_t)e & m);
+  };
+  for (uint32_t c = cs; c < ce; c += 32) {
+    const uint32_t j = c + lane;
+    uint32_t ab = 0, len = 0, ob = 0, oe = 0, walk_u = 0;
+    if (j < ce) {
+      const uint32_t v = g.col[j];
+      const uint64_t va = g.rp[v], vb = g.rp[v + 1];
+      const uint32_t vbs = rp_blk(va), vbe = rp_blk(vb);
+      uint32_t lo = 0, hi = nbu;  // position of v's block in u's row
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((uint32_t)(urow[mid] >> 32) < (v >> 5))
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const uint32_t ta = nbu - lo, tb = vbe - vbs;
+      walk_u = ta <= tb ? 1u : 0u;
+      if (walk_u) {
+        ab = lo, len = ta, ob = vbs, oe = vbe;
+      } else {
+        ab = vbs, len = tb, ob = lo, oe = nbu;
+      }
+    }
+    uint32_t longm = __ballot_sync(kFull, len >= kLong);
+    while (longm) {
+      const int s = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const uint32_t sab = __shfl_sync(kFull, ab, s), slen = __shfl_sync(kFull, len, s);
+      const uint32_t sob = __shfl_sync(kFull, ob, s), soe = __shfl_sync(kFull, oe, s);
+      const bool sw = __shfl_sync(kFull, walk_u, s) != 0;
+      for (uint32_t k = lane; k < slen; k += 32) acc += item(sab + k, sw, sob, soe);
+    }
+    const uint32_t sl = len >= kLong ? 0u : len;
+    const uint32_t incl = warp_inclusive_sum(sl);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t excl = incl - sl;
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t t = base + lane;
+      uint32_t s = 0;
+#pragma unroll
+      for (uint32_t st = 16; st >= 1; st >>= 1) {
+        const uint32_t x = __shfl_sync(kFull, incl, s + st - 1);
+        if (x <= t) s += st;
+      }
+      const uint32_t sab = __shfl_sync(kFull, ab, s), sex = __shfl_sync(kFull, excl, s);
+      const uint32_t sob = __shfl_sync(kFull, ob, s), soe = __shfl_sync(kFull, oe, s);
+      const bool sw = __shfl_sync(kFull, walk_u, s) != 0;
+      if (t < total) acc += item(sab + (t - sex), sw, sob, soe);
+    }
+  }
+  return acc;
+}
+
 __device__ __forceinline__ void push_row(DeviceStats* stats, int which, uint32_t* list, uint32_t u) {
   const uint32_t i = atomicAdd(&stats->overflow[which], 1u);
   list[i] = u;
@@ -162,12 +246,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
                                                                     DeviceStats* stats, uint32_t* __restrict__ ovf_cta,
                                                                     unsigned long long* per_graph,
                                                                     unsigned long long* block_ns,
-                                                                    const uint32_t* __restrict__ heavy) {
+                                                                    const uint32_t* __restrict__ heavy,
+                                                                    int do_pieces) {
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
   __shared__ uint32_t s_row;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* tbl = smem[w];
-  uint32_t* lst = reinterpret_cast<uint32_t*>(smem[w]);
+
   const uint32_t p0 = piece_off[V], len = piece_off[V + 1] - p0;
   uint64_t acc = 0;
   // Phase 1 (first kernel only): rows too wide for a warp's slice, one at a
@@ -208,10 +293,15 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
     }
     __syncthreads();
   }
+  if (!do_pieces) {
+    acc = warp_sum(acc);
+    if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+    return;
+  }
   uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
   bool cur_ok = false;
   int logb = 0;
-  uint32_t bmin = 0, bmax = 0, d = 0, last = 0;
+  uint32_t bmin = 0, bmax = 0, d = 0;
   for (;;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurVariant0 + V], kGrab);
@@ -229,12 +319,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         __syncwarp();
         cur = u;
         if (V == TRIBIT_VARIANT_MERGE) {
-          d = re - rs;
-          cur_ok = d <= kWarpMaxList;
-          if (cur_ok) {
-            for (uint32_t k = lane; k < d; k += 32) lst[k] = g.col[rs + k];
-            last = g.col[re - 1];
-          }
+          const uint32_t bs = rp_blk(a), be = rp_blk(b);
+          d = be - bs;  // u's bit-row length
+          cur_ok = d <= kWarpMaxBlocks;
+          if (cur_ok)
+            for (uint32_t k = lane; k < d; k += 32) tbl[k] = g.bent[bs + k];
         } else {
           const uint32_t bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
           cur_ok = nb <= kWarpMaxBlocks;
@@ -257,19 +346,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       const uint32_t cs = rs + first, ce = min(cs + kPieceNeighbours, re);
       uint64_t racc;
       if (V == TRIBIT_VARIANT_MERGE) {
-        racc = sweep<false>(g, cs, ce, 0, 1, [&](uint32_t k, uint32_t c) -> uint32_t {
-          const uint32_t x = g.col[k];
-          if (x > last) return 0u;
-          uint32_t lo = c - rs + 1, hi = d;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (lst[mid] < x)
-              lo = mid + 1;
-            else
-              hi = mid;
-          }
-          return (lo < d && lst[lo] == x) ? 1u : 0u;
-        });
+        racc = sweep_merge(g, tbl, d, cs, ce);
       } else {
         const BitmapProbe probe{tbl, logb, bmin, bmax};
         racc = sweep<true>(g, cs, ce, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
@@ -301,13 +378,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
 // edge. Row blocks that do not fit fall back to the bitmap sweep in place.
 
 constexpr int kTileStride = kTileMaxK + 4;      // padded: fragment loads hit 32 distinct banks
-constexpr int kTileMaxV = kTileMaxK * 32;
 constexpr int kTileWarps = 4;
 struct TileSmem {
   uint32_t a[32 * kTileStride];                 // also the fallback hash table (4 KiB used)
   uint32_t b[8 * kTileStride];
-  uint32_t vmask[kTileMaxK];
-  uint16_t vlist[kTileMaxV];
+  uint32_t vmask[kTileMaxK];                    // OR of the A rows: the neighbour set of R
 };
 
 __device__ __forceinline__ void mma_b1(int (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
@@ -404,27 +479,38 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
           }
         }
         __syncwarp();
-        // Neighbour set V: OR of the A rows, listed in column order.
-        uint32_t nv_total = 0;
-        for (uint32_t w0 = 0; w0 < KP; w0 += 32) {
-          const uint32_t w = w0 + lane;
+        // Neighbour set V: OR of the A rows.
+        for (uint32_t w = lane; w < KP; w += 32) {
           uint32_t m = 0;
           if (w < K)
             for (uint32_t r = 0; r < 32; ++r) m |= sm.a[r * kTileStride + w];
-          const uint32_t c = __popc(m);
-          const uint32_t incl = warp_inclusive_sum(c);
-          uint32_t pos = nv_total + incl - c;
-          for (uint32_t bits = m; bits; bits &= bits - 1) sm.vlist[pos++] = (uint16_t)(w * 32 + __ffs(bits) - 1);
-          nv_total += __shfl_sync(kFull, incl, 31);
+          sm.vmask[w] = m;
         }
         __syncwarp();
         int rowsum[4] = {0, 0, 0, 0};  // rows grp, grp + 8, 16 + grp, 24 + grp
-        for (uint32_t j0 = 0; j0 < nv_total; j0 += 8) {
+        uint32_t cw = 0, cbits = sm.vmask[0];  // warp-uniform cursor over V's set bits
+        for (;;) {
+          // Next 8 neighbours, as column offsets from lo * 32 (0xFFFF = none).
+          uint32_t vc[8];
+          uint32_t nv = 0;
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            while (cbits == 0 && cw + 1 < K) cbits = sm.vmask[++cw];
+            vc[jj] = 0xFFFFu;
+            if (cbits) {
+              vc[jj] = cw * 32 + __ffs(cbits) - 1;
+              cbits &= cbits - 1;
+              ++nv;
+            }
+          }
+          if (nv == 0) break;
           for (uint32_t i = lane; i < 8 * kTileStride; i += 32) sm.b[i] = 0u;
           __syncwarp();
-          // B tile: the 8 neighbours' masks on [lo, lo + K).
-          for (uint32_t jj = 0; jj < 8 && j0 + jj < nv_total; ++jj) {
-            const uint32_t v = lo * 32 + sm.vlist[j0 + jj];
+          // B tile: the neighbours' masks on [lo, lo + K).
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            if (vc[jj] == 0xFFFFu) continue;
+            const uint32_t v = lo * 32 + vc[jj];
             const uint64_t va = g.rp[v], vb = g.rp[v + 1];
             const uint32_t vbs = rp_blk(va), vn = min(rp_blk(vb) - vbs, K);
             for (uint32_t k = lane; k < vn; k += 32) {
@@ -444,11 +530,14 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
                    a0p[24 * kTileStride + 4], b0, b1);
           }
           // D[row][col]: c[0] (grp, 2t), c[1] (grp, 2t+1), c[2] (grp+8, 2t), c[3] (grp+8, 2t+1).
+          uint32_t vcol[2] = {vc[0], vc[1]};
+#pragma unroll
+          for (int q = 1; q < 4; ++q)
+            if (tig == (uint32_t)q) vcol[0] = vc[2 * q], vcol[1] = vc[2 * q + 1];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const uint32_t col = 2 * tig + (q & 1);
-            if (j0 + col >= nv_total) continue;
-            const uint32_t vo = sm.vlist[j0 + col];
+            const uint32_t vo = vcol[q & 1];
+            if (vo == 0xFFFFu) continue;
             const uint32_t ra = grp + ((q >> 1) ? 8 : 0), rbb = ra + 16;
             if ((sm.a[ra * kTileStride + (vo >> 5)] >> (vo & 31)) & 1u) rowsum[q >> 1] += c0[q];
             if ((sm.a[rbb * kTileStride + (vo >> 5)] >> (vo & 31)) & 1u) rowsum[2 + (q >> 1)] += c1[q];
@@ -823,21 +912,30 @@ LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stat
   TB_CUDA(cudaMemsetAsync(&stats->triangles, 0, sizeof(stats->triangles), st));
   uint32_t* ovf_cta = s.overflow;
   uint32_t* ovf_global = s.overflow + s.overflow_cap;
+  if (cfg.variant_start) {
+    // Timing mode: the heavy rows (the same for every variant) run first, on
+    // their own, so the events bracket only the variant kernels.
+    k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
+        g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, nullptr, s.heavy, 0);
+    TB_LAUNCH_CHECK();
+    TB_CUDA(cudaEventRecord(cfg.variant_start, st));
+  }
   k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy);
+      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, cfg.variant_start ? nullptr : s.heavy, 1);
   TB_LAUNCH_CHECK();
-  k_tiles_mma<<<(unsigned)(sms * 3), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
+  k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
       g, s.variant_of, s.num_row_blocks, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
-                                                                               per_graph, cfg.block_ns, nullptr);
+                                                                               per_graph, cfg.block_ns, nullptr, 1);
   TB_LAUNCH_CHECK();
   k_rows_cta<<<(unsigned)sms, kCtaThreads, sizeof(uint64_t) << kCtaLogSlots, st>>>(g, ovf_cta, stats, ovf_global,
                                                                                    per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
   TB_LAUNCH_CHECK();
-  info.ctas = 2ull * warp_grid + 5ull * sms;
+  if (cfg.variant_stop) TB_CUDA(cudaEventRecord(cfg.variant_stop, st));
+  info.ctas = 2ull * warp_grid + 7ull * sms;
   info.kernels = 5;
   return info;
 }

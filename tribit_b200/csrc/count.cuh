@@ -48,6 +48,8 @@ struct CountConfig {
   int ctas_per_sm = 0;  // 0 = default
   int num_sms = 148;
   unsigned long long* block_ns = nullptr;  // optional: per-row-block SM cycles, summed over pieces
+  cudaEvent_t variant_start = nullptr;     // optional (timing mode): heavy rows run first, on
+  cudaEvent_t variant_stop = nullptr;      // their own; these events bracket the variant kernels
 };
 
 Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E);

@@ -492,7 +492,7 @@ tribit_status tribit_block_features(tribit_context* c, float* out, uint64_t cap,
 }
 
 tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_out, uint64_t cap,
-                                 uint64_t* triangles_out) {
+                                 uint64_t* triangles_out, float* variant_ms) {
   if (!c || !c->prepared || variant < 0 || variant >= TRIBIT_NUM_VARIANTS) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     DeviceGuard dg(c->device);
@@ -511,12 +511,15 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     cfg.num_sms = c->num_sms;
     cfg.ctas_per_sm = c->opts.ctas_per_sm;
     cfg.block_ns = ns;
+    cfg.variant_start = c->ev[0];
+    cfg.variant_stop = c->ev[1];
     tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
     std::vector<unsigned long long> h(nrb + 1);
     TB_CUDA(cudaMemcpyAsync(h.data(), ns, nrb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
     TB_CUDA(cudaMemcpyAsync(c->h_stats, c->prep.stats, sizeof(tb::DeviceStats), cudaMemcpyDeviceToHost, c->st));
     TB_CUDA(cudaStreamSynchronize(c->st));
     if (triangles_out) *triangles_out = c->h_stats->triangles;
+    if (variant_ms) TB_CUDA(cudaEventElapsedTime(variant_ms, c->ev[0], c->ev[1]));
     if (cycles_out)
       for (uint64_t i = 0; i < nrb; ++i) cycles_out[i] = (float)h[i];
     tb::apply_dispatch(c, c->st);

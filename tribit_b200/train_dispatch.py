@@ -4,13 +4,14 @@ For each training graph (generated here, with seeds disjoint from the
 benchmark's) the counter prepares the graph on the GPU, reads the 16
 features of every 32-row block (tribit_block_features), then counts the whole
 graph once per variant with every row block forced onto that variant,
-recording the SM cycles each row block took (tribit_block_times). The MLP
-(16 -> 64 -> 64 -> 3) is trained on the GPU by the library's own forward,
-backward and Adam kernels (tribit_model_train) to predict log2(1 + cycles) of
-each variant, and is evaluated on a held-out graph: total cycles of the
-plain dispatcher's choice, of the MLP's choice and of the per-block best
-(regret = chosen - best), plus the measured counting time under each
-dispatcher.
+recording the SM cycles each row block took and the device time of the
+variant's kernels (tribit_block_times); cycles scaled to that time give each
+row block's cost under each variant. The MLP (16 -> 64 -> 64 -> 3) is trained
+on the GPU by the library's own forward, backward and Adam kernels
+(tribit_model_train) to predict log2(1 + cost in ns) of each variant, and is
+evaluated on a held-out graph: total cost of the plain dispatcher's choice,
+of the MLP's choice and of the per-block best (regret = chosen - best), plus
+the measured counting time under each dispatcher.
 
   python -m tribit_b200.train_dispatch [--out tribit_b200/models/dispatch_mlp.bin] [--quick]
 """
@@ -65,21 +66,29 @@ def holdout_graph(quick: bool):
 
 
 def collect(n, e, repeats: int = 2):
+    """Features and per-row-block cost (ns) of each variant.
+
+    A row block's SM cycles measure how long its warp worked, not what it cost
+    the machine: a variant whose kernel keeps fewer warps resident per SM
+    finishes fewer blocks per second at the same cycles per block. So each
+    variant's cycles are scaled to its measured device time: cost of block b
+    = cycles_b / sum of cycles * time of the variant kernels."""
     import torch
     d = torch.from_numpy(e.view(np.int64)).cuda()
     with tb.Counter(dispatch="plain") as c:
         c.prepare_device(d.data_ptr(), d.numel(), n)
         x = c.block_features()
-        times, tri = [], set()
+        costs, tri = [], set()
         for v in tb.VARIANTS:
-            runs = []
+            best = None
             for _ in range(repeats):
-                t, count = c.block_times(v)
-                runs.append(t)
+                cyc, count, ms = c.block_times(v)
                 tri.add(count)
-            times.append(np.minimum.reduce(runs))
+                cost = cyc / max(float(cyc.sum()), 1.0) * ms * 1e6
+                best = cost if best is None or cost.sum() < best.sum() else best
+            costs.append(best)
         assert len(tri) == 1, "variants disagree on the count"
-    t = np.stack(times, 1)
+    t = np.stack(costs, 1)
     keep = t.max(1) > 0
     return x[keep], t[keep], x, t
 
@@ -134,7 +143,7 @@ def main():
         xs.append(x)
         ys.append(np.log2(1.0 + t))
         print(json.dumps({"graph": name, "row_blocks": int(x.shape[0]), "seconds": round(time.time() - t0, 1),
-                          "cycles_per_variant": dict(zip(tb.VARIANTS, map(float, t.sum(0))))}), flush=True)
+                          "ms_per_variant": dict(zip(tb.VARIANTS, [float(v) / 1e6 for v in t.sum(0)]))}), flush=True)
     X = np.concatenate(xs).astype(np.float32)
     Y = np.concatenate(ys).astype(np.float32)
     norm = np.concatenate([X.mean(0), X.std(0) + 1e-3, Y.mean(0), Y.std(0) + 1e-3]).astype(np.float32)
@@ -153,9 +162,9 @@ def main():
     best = ht.min(1).sum()
     report = {
         "train_rows": int(X.shape[0]), "final_loss": loss, "holdout": hname,
-        "holdout_cycles": {"best": float(best), "plain": float(ht[rows, plain].sum()),
-                           "learned": float(ht[rows, learned].sum()),
-                           **{f"all_{v}": float(ht[:, i].sum()) for i, v in enumerate(tb.VARIANTS)}},
+        "holdout_cost_ms": {"best": float(best) / 1e6, "plain": float(ht[rows, plain].sum()) / 1e6,
+                            "learned": float(ht[rows, learned].sum()) / 1e6,
+                            **{f"all_{v}": float(ht[:, i].sum()) / 1e6 for i, v in enumerate(tb.VARIANTS)}},
         "learned_picks": dict(zip(tb.VARIANTS, np.bincount(learned, minlength=3).tolist())),
         "plain_picks": dict(zip(tb.VARIANTS, np.bincount(plain, minlength=3).tolist())),
     }
