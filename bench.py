@@ -12,7 +12,11 @@ host entries: H2D copy, preprocessing, counting and the D2H result inside.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload rmat24|rmat22|rmat20|chung_lu|planted]
-                  [--dispatch auto|plain|learned|bitmap|merge|mma]
+                  [--dispatch auto|plain|learned|bitmap|merge|mma] [--no-batch]
+
+config.batch reports the batched workload: 4,096 graphs (n log-uniform in
+[64, 65536], Erdos-Renyi or Chung-Lu by seed) counted by one persistent
+launch replayed from a CUDA graph (graphs/s), against one count per graph.
 
 Multi-GPU: the counter has no cross-GPU exchange, so N GPUs run N independent
 replicas (seed + rank), one process each under torchrun; value is the sum of
@@ -157,6 +161,65 @@ def cpu_baseline(entries, n, m, target_s=15.0, steps=1):
     return out, threads
 
 
+def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=4096, seed=4096, steps=5,
+                      per_graph_sample=256):
+    """The batched workload: num_graphs graphs (n log-uniform in [64, 65536],
+    Erdos-Renyi or Chung-Lu by seed) counted in one persistent launch replayed
+    from a CUDA graph, against counting graphs one at a time."""
+    e, off, nn = tb.gen_batch(num_graphs, seed=seed)
+    pinned = torch.empty(e.size, dtype=torch.int64, pin_memory=True)
+    pinned.numpy()[:] = e.view(np.int64)
+    host = pinned.numpy().view(np.uint64)
+    c = tb.Counter(device=local, dispatch=dispatch)
+    if dispatch == "learned":
+        c.load_model(model_path)
+    counts, r = c.count_batch(host, off, nn)  # sizes the arena, prepares the batch
+    t0 = time.perf_counter()
+    counts, r = c.count_batch(host, off, nn)
+    e2e_s = time.perf_counter() - t0
+    tune = c.autotune(reps=2)
+    c.capture_count()
+    s = torch.cuda.Stream(device=local)
+    c.set_stream(s.cuda_stream)
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        c.launch_count()
+        b.record(s)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    replay = c.batch_counts(num_graphs)
+    assert np.array_equal(replay, counts), "graph replay changed the per-graph counts"
+    c.close()
+    # One graph at a time (a strided sample), same library, same stream model.
+    d = torch.from_numpy(e.view(np.int64)).to(f"cuda:{local}")
+    c1 = tb.Counter(device=local, dispatch=dispatch)
+    if dispatch == "learned":
+        c1.load_model(model_path)
+    idx = np.linspace(0, num_graphs - 1, per_graph_sample).astype(int)
+    k_ms, e2e_one = 0.0, 0.0
+    for g in idx:
+        lo, hi = int(off[g]), int(off[g + 1])
+        c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))  # sizes the arena
+        t1 = time.perf_counter()
+        rg = c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))
+        e2e_one += time.perf_counter() - t1
+        k_ms += rg.kernel_ms
+        assert rg.triangles == int(counts[g]), f"graph {g}: batch {counts[g]} vs single {rg.triangles}"
+    c1.close()
+    scale = num_graphs / per_graph_sample
+    batched_ms = statistics.median(ms)
+    return {
+        "graphs": num_graphs, "entries": int(e.size), "edges": int(r.edges), "triangles": int(counts.sum()),
+        "batched_count_ms": batched_ms, "graphs_per_s_batched": num_graphs / (batched_ms / 1e3),
+        "graphs_per_s_per_graph_launches": num_graphs / (k_ms * scale / 1e3),
+        "e2e_graphs_per_s_batched": num_graphs / e2e_s,
+        "e2e_graphs_per_s_per_graph": num_graphs / (e2e_one * scale),
+        "per_graph_sample": per_graph_sample, "tuning": tune.as_dict(), "cuda_graph": True,
+    }
+
+
 def run_reference(args, spec, rank, world):
     import tribit_b200 as tb
     if rank != 0:
@@ -192,6 +255,7 @@ def main():
     ap.add_argument("--dispatch", default="auto")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -306,6 +370,10 @@ def main():
     achieved = b_alg / (ms_per_step / 1e3) / 1e9
     traffic = profiled_traffic(args.workload)
 
+    batch = None
+    if not args.no_batch:
+        batch = batch_measurement(tb, np, torch, local, dispatch, model_path, seed=4096 + rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         steps, threads = cpu_baseline(entries, n, m, steps=1)
@@ -325,7 +393,8 @@ def main():
                        "preprocess_ms": prep.preprocess_ms, "gen_s": round(gen_s, 2),
                        "row_blocks_by_variant": dict(zip(tb.VARIANTS, res.row_blocks_by_variant)),
                        "per_mode_edges_per_s": {k: world * v[1].edges / (sum(v[2]) / len(v[2]) / 1e3)
-                                                for k, v in results.items()}},
+                                                for k, v in results.items()},
+                       "batch": batch},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,

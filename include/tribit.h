@@ -121,6 +121,27 @@ tribit_status tribit_prepare_device(tribit_context* ctx, const uint64_t* d_entri
 tribit_status tribit_launch_count(tribit_context* ctx);
 tribit_status tribit_read_count(tribit_context* ctx, tribit_result* out);
 
+/* ---- launch tuning and CUDA-graph replay (no counterpart in the reference) - */
+typedef struct tribit_tuning {
+  int ctas_per_sm;      /* CTAs per SM of the warp-per-piece kernels; 0 = default (6) */
+  uint32_t piece_width; /* neighbours per work piece: a multiple of 32, >= 32 (default 64) */
+  float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles (default 64) */
+  float count_ms;       /* tribit_autotune: measured counting time of this setting */
+} tribit_tuning;
+tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);
+/* Applies to later calls, and rebuilds the schedule of the prepared graph. */
+tribit_status tribit_set_tuning(tribit_context* ctx, const tribit_tuning* in);
+/* Times `reps` counting launches of the prepared graph for each setting of a
+ * small grid (CTAs/SM x piece width x tile threshold), keeps the fastest
+ * (median) and returns it. Counts stay exact under every setting. */
+tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning* best);
+/* Captures the counting launch of the prepared graph (or batch) into a CUDA
+ * graph; tribit_launch_count then replays it with one graph launch. Preparing
+ * another input or changing the tuning drops the capture. */
+tribit_status tribit_capture_count(tribit_context* ctx);
+/* After tribit_count_batch: per-graph counts of the latest counting launch. */
+tribit_status tribit_read_batch_counts(tribit_context* ctx, uint64_t* triangles_out, uint32_t num_graphs);
+
 /* ---- Matrix Market ------------------------------------------------------ */
 /* Reads a coordinate .mtx with the reference's semantics (tribit.cu:228-269):
  * banner line, '%' lines skipped, "rows cols nnz", rows must equal cols,
@@ -209,6 +230,13 @@ tribit_status tribit_gen_chung_lu(uint32_t n, uint64_t n_entries, double beta, d
 tribit_status tribit_gen_planted(uint32_t communities, uint32_t size, double p_in, uint32_t inter_per_vertex,
                                  uint64_t seed, uint64_t* out, uint64_t* n_entries);
 tribit_status tribit_write_mtx(const char* path, uint64_t num_nodes, const uint64_t* entries, uint64_t n_entries);
+/* The batched workload: num_graphs graphs, graph g with n log-uniform in
+ * [min_n, max_n] and, by seed, Erdos-Renyi or Chung-Lu (exponent 2.1-2.8),
+ * mean degree uniform in [8, 64], n * degree / 2 entries. Call with
+ * entries == NULL to fill num_nodes[num_graphs] and entry_offsets[num_graphs+1]
+ * only, then again with entries[entry_offsets[num_graphs]]. */
+tribit_status tribit_gen_batch(uint32_t num_graphs, uint32_t min_n, uint32_t max_n, uint64_t seed, uint32_t* num_nodes,
+                               uint64_t* entry_offsets, uint64_t* entries);
 
 #ifdef __cplusplus
 }

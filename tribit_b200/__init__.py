@@ -91,6 +91,21 @@ _decl("tribit_model_train", ctypes.c_int, _p, _p, _p, _u64, _u32, _u32, ctypes.c
 _decl("tribit_block_features", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
 _decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POINTER(_u64),
       ctypes.POINTER(ctypes.c_float))
+class Tuning(ctypes.Structure):
+    """tribit_tuning: launch parameters of the counting kernels."""
+    _fields_ = [("ctas_per_sm", ctypes.c_int), ("piece_width", _u32), ("tile_min_nnz", ctypes.c_float),
+                ("count_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_decl("tribit_get_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
+_decl("tribit_set_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
+_decl("tribit_autotune", ctypes.c_int, _p, _u32, ctypes.POINTER(Tuning))
+_decl("tribit_capture_count", ctypes.c_int, _p)
+_decl("tribit_read_batch_counts", ctypes.c_int, _p, _p, _u32)
+_decl("tribit_gen_batch", ctypes.c_int, _u32, _u32, _u32, _u64, _p, _p, _p)
 _decl("tribit_count_edges_noalloc", ctypes.c_int, _p, _u64, _u64, _p, _p)
 _decl("tribit_noalloc_scratch_bytes", _u64)
 _decl("tribit_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64, _p)
@@ -178,6 +193,29 @@ class Counter:
 
     def load_model(self, path: str):
         _check(lib.tribit_model_load(self._h, path.encode()), self._h)
+
+    # -- tuning and CUDA-graph replay ----------------------------------------
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        _check(lib.tribit_get_tuning(self._h, ctypes.byref(t)), self._h)
+        return t
+
+    def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 64.0):
+        t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0)
+        _check(lib.tribit_set_tuning(self._h, ctypes.byref(t)), self._h)
+
+    def autotune(self, reps: int = 2) -> Tuning:
+        t = Tuning()
+        _check(lib.tribit_autotune(self._h, reps, ctypes.byref(t)), self._h)
+        return t
+
+    def capture_count(self):
+        _check(lib.tribit_capture_count(self._h), self._h)
+
+    def batch_counts(self, num_graphs: int) -> np.ndarray:
+        out = np.zeros(num_graphs, dtype=np.uint64)
+        _check(lib.tribit_read_batch_counts(self._h, out.ctypes.data, num_graphs), self._h)
+        return out
 
     # -- learned dispatcher ------------------------------------------------
     def model_init(self, norm, seed: int = 1):
@@ -329,6 +367,16 @@ def gen_chung_lu(n: int, n_entries: int, beta: float, max_degree: float, seed: i
     out = np.empty(n_entries, dtype=np.uint64)
     _check(lib.tribit_gen_chung_lu(n, n_entries, beta, max_degree, seed, out.ctypes.data))
     return out
+
+
+def gen_batch(num_graphs: int, seed: int = 1, min_n: int = 64, max_n: int = 65536):
+    """The batched workload -> (entries, entry_offsets, num_nodes)."""
+    nn = np.zeros(num_graphs, dtype=np.uint32)
+    off = np.zeros(num_graphs + 1, dtype=np.uint64)
+    _check(lib.tribit_gen_batch(num_graphs, min_n, max_n, seed, nn.ctypes.data, off.ctypes.data, None))
+    e = np.empty(int(off[-1]), dtype=np.uint64)
+    _check(lib.tribit_gen_batch(num_graphs, min_n, max_n, seed, nn.ctypes.data, off.ctypes.data, e.ctypes.data))
+    return e, off, nn
 
 
 def gen_planted(communities: int, size: int, p_in: float, inter_per_vertex: int, seed: int = 1) -> np.ndarray:

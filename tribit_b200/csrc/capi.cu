@@ -4,6 +4,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "context.h"
@@ -76,16 +77,18 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
     pin.eoff = L.eoff;
     pin.voff = L.voff;
   }
+  tb::drop_graph(c);
   tb::prepare_graph(c->arena, pin, st, &c->prep);
   c->sched = tb::take_schedule(c->arena, in.n, in.E);
   tb::apply_dispatch(c, st);
   c->per_graph = L.per_graph;
+  c->num_graphs = G;
   c->prepared = true;
   TB_CUDA(cudaEventRecord(c->ev[2], st));
   if (count) {
     tb::CountConfig cfg;
     cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->opts.ctas_per_sm;
+    cfg.ctas_per_sm = c->ctas_per_sm;
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, L.per_graph, cfg, st);
   }
   TB_CUDA(cudaEventRecord(c->ev[3], st));
@@ -174,6 +177,7 @@ tribit_status tribit_create(const tribit_options* opts, tribit_context** out) {
   if (!c) return TRIBIT_ERR_OUT_OF_MEMORY;
   c->opts = o;
   c->device = o.device;
+  c->ctas_per_sm = o.ctas_per_sm;
   tribit_status st = guarded(c, [&] {
     DeviceGuard dg(c->device);
     TB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -196,6 +200,7 @@ void tribit_destroy(tribit_context* c) {
     DeviceGuard dg(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     c->arena.release();
+    tb::drop_graph(c);
     c->train_arena.release();
     c->timing_arena.release();
     tb::model_free(c->model);
@@ -260,11 +265,117 @@ tribit_status tribit_launch_count(tribit_context* c) {
   if (!c->prepared) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     DeviceGuard dg(c->device);
+    if (c->graph_exec) {
+      if (c->num_graphs) TB_CUDA(cudaMemsetAsync(c->per_graph, 0, c->num_graphs * sizeof(unsigned long long), c->st));
+      TB_CUDA(cudaGraphLaunch(c->graph_exec, c->st));
+      return;
+    }
     tb::CountConfig cfg;
     cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->opts.ctas_per_sm;
+    cfg.ctas_per_sm = c->ctas_per_sm;
+    if (c->num_graphs) TB_CUDA(cudaMemsetAsync(c->per_graph, 0, c->num_graphs * sizeof(unsigned long long), c->st));
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
   });
+}
+
+tribit_status tribit_capture_count(tribit_context* c) {
+  if (!c || !c->prepared) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    tb::drop_graph(c);
+    tb::CountConfig cfg;
+    cfg.num_sms = c->num_sms;
+    cfg.ctas_per_sm = c->ctas_per_sm;
+    // One ordinary launch first: one-time function attributes are set outside the capture.
+    c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
+    TB_CUDA(cudaStreamSynchronize(c->st));
+    TB_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    try {
+      tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c->st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    TB_CUDA(cudaStreamEndCapture(c->st, &c->graph));
+    TB_CUDA(cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
+  });
+}
+
+tribit_status tribit_read_batch_counts(tribit_context* c, uint64_t* out, uint32_t num_graphs) {
+  if (!c || !c->prepared || !out || num_graphs != c->num_graphs || num_graphs == 0) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    TB_CUDA(cudaMemcpyAsync(out, c->per_graph, num_graphs * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->st));
+    TB_CUDA(cudaStreamSynchronize(c->st));
+  });
+}
+
+tribit_status tribit_get_tuning(tribit_context* c, tribit_tuning* t) {
+  if (!c || !t) return TRIBIT_ERR_INVALID_ARGUMENT;
+  t->ctas_per_sm = c->ctas_per_sm;
+  t->piece_width = c->piece_width;
+  t->tile_min_nnz = c->tile_min_nnz;
+  t->count_ms = 0.f;
+  return TRIBIT_OK;
+}
+
+tribit_status tribit_set_tuning(tribit_context* c, const tribit_tuning* t) {
+  if (!c || !t || t->ctas_per_sm < 0 || t->ctas_per_sm > 32 || t->piece_width < tb::kMinPieceWidth ||
+      t->piece_width % 32 != 0 || t->piece_width > 4096 || !(t->tile_min_nnz >= 0.f))
+    return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->ctas_per_sm = t->ctas_per_sm;
+    c->piece_width = t->piece_width;
+    c->tile_min_nnz = t->tile_min_nnz;
+    if (c->prepared) {
+      DeviceGuard dg(c->device);
+      tb::apply_dispatch(c, c->st);
+      TB_CUDA(cudaStreamSynchronize(c->st));
+    }
+  });
+}
+
+tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* best) {
+  if (!c || !c->prepared || !best) return TRIBIT_ERR_INVALID_ARGUMENT;
+  if (reps == 0) reps = 2;
+  static const int kCtas[] = {4, 6, 7};
+  static const uint32_t kWidths[] = {32, 64, 128};
+  static const float kTile[] = {64.f, 1e30f};
+  tribit_tuning cur{}, found{};
+  found.count_ms = 1e30f;
+  for (int ctas : kCtas)
+    for (uint32_t w : kWidths)
+      for (float tile : kTile) {
+        cur.ctas_per_sm = ctas;
+        cur.piece_width = w;
+        cur.tile_min_nnz = tile;
+        tribit_status st = tribit_set_tuning(c, &cur);
+        if (st != TRIBIT_OK) return st;
+        st = guarded(c, [&] {
+          DeviceGuard dg(c->device);
+          tb::CountConfig cfg;
+          cfg.num_sms = c->num_sms;
+          cfg.ctas_per_sm = c->ctas_per_sm;
+          tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);  // warm
+          std::vector<float> ms(reps);
+          for (uint32_t r = 0; r < reps; ++r) {
+            TB_CUDA(cudaEventRecord(c->ev[0], c->st));
+            tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
+            TB_CUDA(cudaEventRecord(c->ev[1], c->st));
+            TB_CUDA(cudaEventSynchronize(c->ev[1]));
+            ms[r] = elapsed(c->ev[0], c->ev[1]);
+          }
+          std::sort(ms.begin(), ms.end());
+          cur.count_ms = ms[reps / 2];
+        });
+        if (st != TRIBIT_OK) return st;
+        if (cur.count_ms < found.count_ms) found = cur;
+      }
+  tribit_status st = tribit_set_tuning(c, &found);
+  *best = found;
+  return st;
 }
 
 tribit_status tribit_read_count(tribit_context* c, tribit_result* out) {

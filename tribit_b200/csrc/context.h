@@ -26,6 +26,13 @@ struct tribit_context {
   tb::LaunchInfo launch{};
   cudaEvent_t ev[6] = {};
   tb::DeviceStats* h_stats = nullptr;  // pinned
+  // Tuned launch parameters (tribit_set_tuning / tribit_autotune).
+  int ctas_per_sm = 0;
+  uint32_t piece_width = 64;
+  float tile_min_nnz = 64.f;
+  uint32_t num_graphs = 0;             // batch size of the prepared input (0: single graph)
+  cudaGraph_t graph = nullptr;         // captured counting launch (tribit_capture_count)
+  cudaGraphExec_t graph_exec = nullptr;
   tb::DeviceModel model{};
   tb::Arena train_arena;               // training batches and activations
   tb::Arena timing_arena;              // per-row-block cycle counters
@@ -68,7 +75,15 @@ tribit_status guarded(tribit_context* ctx, F&& body) {
 }
 
 // Rebuilds the context's schedule for its dispatch mode (learned mode runs the
-// MLP over full features).
+// MLP over full features) with its tuned piece width and tile threshold.
 void apply_dispatch(tribit_context* c, cudaStream_t st);
+
+// Drops a captured counting graph (the schedule it was captured from changed).
+inline void drop_graph(tribit_context* c) {
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  c->graph_exec = nullptr;
+  c->graph = nullptr;
+}
 
 }  // namespace tb

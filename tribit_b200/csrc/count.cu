@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
                                                                     unsigned long long* per_graph,
                                                                     unsigned long long* block_ns,
                                                                     const uint32_t* __restrict__ heavy,
-                                                                    int do_pieces) {
+                                                                    int do_pieces, uint32_t width) {
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
   __shared__ uint32_t s_row;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         if (first == 0 && lane == 0) push_row(stats, kOvfCta, ovf_cta, u);
         continue;
       }
-      const uint32_t cs = rs + first, ce = min(cs + kPieceNeighbours, re);
+      const uint32_t cs = rs + first, ce = min(cs + width, re);
       uint64_t racc;
       if (V == TRIBIT_VARIANT_MERGE) {
         racc = sweep_merge(g, tbl, d, cs, ce);
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 // Row-block features (one warp per row block) and the plain dispatcher's
 // choice. Features are log-scaled so the learned dispatcher sees O(1) inputs.
 __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restrict__ feat,
-                           uint8_t* __restrict__ variant_of, int full) {
+                           uint8_t* __restrict__ variant_of, int full, float tile_min_nnz) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -751,7 +751,7 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
       // share one narrow column range and have enough edges to share
       // neighbours; the bitmap sweep everywhere else.
       uint8_t var = TRIBIT_VARIANT_BITMAP;
-      if (span > 0.f && span <= (float)kTileMaxK && nnz >= 64.f) var = TRIBIT_VARIANT_MMA;
+      if (span > 0.f && span <= (float)kTileMaxK && nnz >= tile_min_nnz) var = TRIBIT_VARIANT_MMA;
       if (mode == TRIBIT_DISPATCH_BITMAP) var = TRIBIT_VARIANT_BITMAP;
       if (mode == TRIBIT_DISPATCH_MERGE) var = TRIBIT_VARIANT_MERGE;
       if (mode == TRIBIT_DISPATCH_MMA) var = TRIBIT_VARIANT_MMA;
@@ -762,12 +762,12 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
 
 // Pieces of row u; rows wider than a warp's table are counted whole in the
 // heavy phase instead and get none.
-__device__ __forceinline__ uint32_t row_pieces(const GraphView& g, uint32_t u) {
+__device__ __forceinline__ uint32_t row_pieces(const GraphView& g, uint32_t u, uint32_t width) {
   if (u >= g.n) return 0u;
   const uint64_t a = g.rp[u], b = g.rp[u + 1];
   const uint32_t d = rp_row(b) - rp_row(a);
   if (d < 2 || rp_blk(b) - rp_blk(a) > kWarpMaxBlocks) return 0u;
-  return (d + kPieceNeighbours - 1) / kPieceNeighbours;
+  return (d + width - 1) / width;
 }
 
 __global__ void k_heavy_flags(GraphView g, uint32_t* __restrict__ flags) {
@@ -789,12 +789,12 @@ __global__ void k_heavy_scatter(GraphView g, const uint32_t* __restrict__ pos, u
 }
 
 // Pieces of each row block (one warp per row block).
-__global__ void k_block_pieces(GraphView g, uint32_t nrb, uint32_t* __restrict__ cnt) {
+__global__ void k_block_pieces(GraphView g, uint32_t nrb, uint32_t* __restrict__ cnt, uint32_t width) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
-    const uint32_t s = warp_sum(row_pieces(g, rb * 32 + lane));
+    const uint32_t s = warp_sum(row_pieces(g, rb * 32 + lane, width));
     if (lane == 0) cnt[rb] = s;
   }
 }
@@ -815,7 +815,7 @@ __global__ void k_piece_segment(const uint32_t* __restrict__ off, uint32_t nrb, 
 
 __global__ void k_piece_scatter(GraphView g, uint32_t nrb, const uint8_t* __restrict__ variant_of, int v,
                                 const uint32_t* __restrict__ off, const uint32_t* __restrict__ piece_off,
-                                uint64_t* __restrict__ pieces) {
+                                uint64_t* __restrict__ pieces, uint32_t width) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -823,10 +823,10 @@ __global__ void k_piece_scatter(GraphView g, uint32_t nrb, const uint8_t* __rest
   for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
     if (variant_of[rb] != v) continue;
     const uint32_t u = rb * 32 + lane;
-    const uint32_t np = row_pieces(g, u);
+    const uint32_t np = row_pieces(g, u, width);
     const uint32_t incl = warp_inclusive_sum(np);
     const uint32_t base = seg + off[rb] + incl - np;
-    for (uint32_t k = 0; k < np; ++k) pieces[base + k] = ((uint64_t)u << 32) | (k * kPieceNeighbours);
+    for (uint32_t k = 0; k < np; ++k) pieces[base + k] = ((uint64_t)u << 32) | (k * width);
   }
 }
 
@@ -837,7 +837,7 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E) {
   const uint32_t nrb = (uint32_t)ceil_div<uint64_t>(n, 32);
   s.num_row_blocks = nrb;
   s.variant_of = ar.take<uint8_t>(nrb + 1);
-  s.piece_cap = n + E / kPieceNeighbours + 64;
+  s.piece_cap = n + E / kMinPieceWidth + 64;
   s.pieces = ar.take<uint64_t>(s.piece_cap);
   s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 2);
   s.heavy = ar.take<uint32_t>(n + 1);
@@ -859,7 +859,7 @@ void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
   const unsigned fblocks = (unsigned)ceil_div<uint64_t>(nrb + 1, 256);
   TB_CUDA(cudaMemsetAsync(s.list_len, 0, TRIBIT_NUM_VARIANTS * sizeof(uint32_t), st));
   if (nrb) {
-    k_block_pieces<<<wblocks, 256, 0, st>>>(g, nrb, s.block_pieces);
+    k_block_pieces<<<wblocks, 256, 0, st>>>(g, nrb, s.block_pieces, s.piece_width);
     TB_LAUNCH_CHECK();
   }
   for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) {
@@ -869,7 +869,8 @@ void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
     k_piece_segment<<<1, 1, 0, st>>>(s.flags, nrb, v, s.piece_off);
     TB_LAUNCH_CHECK();
     if (nrb) {
-      k_piece_scatter<<<wblocks, 256, 0, st>>>(g, nrb, s.variant_of, v, s.flags, s.piece_off, s.pieces);
+      k_piece_scatter<<<wblocks, 256, 0, st>>>(g, nrb, s.variant_of, v, s.flags, s.piece_off, s.pieces,
+                                               s.piece_width);
       TB_LAUNCH_CHECK();
     }
   }
@@ -885,7 +886,8 @@ void compute_features(const GraphView& g, Schedule& s, int mode, bool full_featu
   const uint32_t nrb = s.num_row_blocks;
   if (nrb == 0) return;
   const unsigned blocks = (unsigned)std::min<uint64_t>(ceil_div<uint64_t>(nrb, 8), 148ull * 16);
-  k_features<<<blocks, 256, 0, st>>>(g, nrb, mode, s.features, s.variant_of, full_features ? 1 : 0);
+  k_features<<<blocks, 256, 0, st>>>(g, nrb, mode, s.features, s.variant_of, full_features ? 1 : 0,
+                                     s.tile_min_nnz);
   TB_LAUNCH_CHECK();
 }
 
@@ -916,18 +918,20 @@ LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stat
     // Timing mode: the heavy rows (the same for every variant) run first, on
     // their own, so the events bracket only the variant kernels.
     k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-        g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, nullptr, s.heavy, 0);
+        g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, nullptr, s.heavy, 0, s.piece_width);
     TB_LAUNCH_CHECK();
     TB_CUDA(cudaEventRecord(cfg.variant_start, st));
   }
   k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, cfg.variant_start ? nullptr : s.heavy, 1);
+      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, cfg.variant_start ? nullptr : s.heavy, 1,
+      s.piece_width);
   TB_LAUNCH_CHECK();
   k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
       g, s.variant_of, s.num_row_blocks, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
-                                                                               per_graph, cfg.block_ns, nullptr, 1);
+                                                                               per_graph, cfg.block_ns, nullptr, 1,
+                                                                               s.piece_width);
   TB_LAUNCH_CHECK();
   k_rows_cta<<<(unsigned)sms, kCtaThreads, sizeof(uint64_t) << kCtaLogSlots, st>>>(g, ovf_cta, stats, ovf_global,
                                                                                    per_graph, cfg.block_ns);

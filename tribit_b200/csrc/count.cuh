@@ -9,7 +9,7 @@
 // Work is scheduled in two levels. The dispatcher assigns every 32-row block
 // of the oriented graph one counting variant (row-block features -> plain
 // thresholds or the learned MLP). Each variant's rows are then cut into
-// pieces of at most kPieceNeighbours neighbours, so one heavy row is spread
+// pieces of at most piece_width neighbours, so one heavy row is spread
 // over many warps; the variant kernels are persistent and pull pieces from a
 // device cursor.
 #pragma once
@@ -22,7 +22,7 @@
 namespace tb {
 
 constexpr int kNumFeatures = 16;
-constexpr uint32_t kPieceNeighbours = 64;
+constexpr uint32_t kMinPieceWidth = 32;  // piece_width is a multiple of 32, at least this
 
 struct Schedule {
   uint32_t num_row_blocks = 0;
@@ -40,6 +40,8 @@ struct Schedule {
   uint32_t* overflow = nullptr;    // device, rows deferred to the CTA / global passes
   uint32_t overflow_cap = 0;
   float* features = nullptr;       // device, nrb x kNumFeatures
+  uint32_t piece_width = 64;       // neighbours per piece (tuned)
+  float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
   const void* model = nullptr;     // device MLP parameters for learned dispatch
 };
 

@@ -175,3 +175,77 @@ extern "C" tribit_status tribit_write_mtx(const char* path, uint64_t num_nodes, 
   std::fwrite(buf.data(), 1, buf.size(), f);
   return std::fclose(f) == 0 ? TRIBIT_OK : TRIBIT_ERR_IO;
 }
+
+namespace {
+
+struct BatchGraph {
+  uint32_t n;
+  uint64_t entries;
+  bool chung_lu;
+  double beta;
+  uint64_t seed;
+};
+
+// Graph g of the batched workload, drawn from stream `seed`.
+BatchGraph batch_graph(uint64_t seed, uint32_t g, uint32_t min_n, uint32_t max_n) {
+  BatchGraph b;
+  const uint64_t s = tb_rand(seed, g);
+  const double u1 = tb_unit(tb_rand(s, 1)), u2 = tb_unit(tb_rand(s, 2)), u3 = tb_unit(tb_rand(s, 3)),
+               u4 = tb_unit(tb_rand(s, 4));
+  const double lo = std::log((double)min_n), hi = std::log((double)max_n);
+  b.n = (uint32_t)std::min<double>(max_n, std::floor(std::exp(lo + (hi - lo) * u1)));
+  if (b.n < min_n) b.n = min_n;
+  const double deg = 8.0 + 56.0 * u3;
+  b.entries = (uint64_t)(b.n * deg / 2.0);
+  b.chung_lu = u2 >= 0.5;
+  b.beta = 2.1 + 0.7 * u4;
+  b.seed = tb_rand(s, 5);
+  return b;
+}
+
+}  // namespace
+
+extern "C" tribit_status tribit_gen_batch(uint32_t num_graphs, uint32_t min_n, uint32_t max_n, uint64_t seed,
+                                          uint32_t* num_nodes, uint64_t* entry_offsets, uint64_t* entries) {
+  if (num_graphs == 0 || min_n < 2 || max_n < min_n || !num_nodes || !entry_offsets) return TRIBIT_ERR_INVALID_ARGUMENT;
+  entry_offsets[0] = 0;
+  for (uint32_t g = 0; g < num_graphs; ++g) {
+    const BatchGraph b = batch_graph(seed, g, min_n, max_n);
+    num_nodes[g] = b.n;
+    entry_offsets[g + 1] = entry_offsets[g] + b.entries;
+  }
+  if (!entries) return TRIBIT_OK;
+  // Graphs are independent: hand them out to host threads one at a time.
+  std::atomic<uint32_t> next{0};
+  auto work = [&] {
+    std::vector<double> w, cdf;
+    for (uint32_t g; (g = next.fetch_add(1)) < num_graphs;) {
+      const BatchGraph b = batch_graph(seed, g, min_n, max_n);
+      uint64_t* out = entries + entry_offsets[g];
+      if (!b.chung_lu) {
+        for (uint64_t i = 0; i < b.entries; ++i) out[i] = tb_er_edge(b.seed, i, b.n);
+        continue;
+      }
+      // Chung-Lu weights (i + 1)^(-1 / (beta - 1)), clipped at an expected
+      // degree of sqrt(2 * entries) (the structural cut-off).
+      w.assign(b.n, 0.0);
+      cdf.assign(b.n, 0.0);
+      const double ex = -1.0 / (b.beta - 1.0);
+      for (uint32_t i = 0; i < b.n; ++i) w[i] = std::pow((double)i + 1.0, ex);
+      const double max_deg = std::sqrt(2.0 * (double)b.entries);
+      for (int it = 0; it < 8; ++it) {
+        double s = 0;
+        for (double x : w) s += x;
+        const double cap = max_deg * s / (2.0 * (double)b.entries);
+        for (double& x : w) x = std::min(x, cap);
+      }
+      double s = 0;
+      for (uint32_t i = 0; i < b.n; ++i) cdf[i] = (s += w[i]);
+      for (uint64_t i = 0; i < b.entries; ++i) out[i] = tb_chung_lu_edge(b.seed, i, cdf.data(), b.n);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < host_threads(); ++t) th.emplace_back(work);
+  for (auto& x : th) x.join();
+  return TRIBIT_OK;
+}

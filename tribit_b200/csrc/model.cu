@@ -333,6 +333,9 @@ void model_dispatch(const DeviceModel& m, const float* features, uint32_t nrb, u
 
 void apply_dispatch(tribit_context* c, cudaStream_t st) {
   const int mode = c->opts.dispatch;
+  c->sched.piece_width = c->piece_width;
+  c->sched.tile_min_nnz = c->tile_min_nnz;
+  drop_graph(c);
   if (mode == TRIBIT_DISPATCH_LEARNED) {
     require_model(c);
     compute_features(c->prep.view, c->sched, TRIBIT_DISPATCH_PLAIN, true, st);
@@ -509,7 +512,7 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     tb::build_pieces(c->prep.view, c->sched, c->st);
     tb::CountConfig cfg;
     cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->opts.ctas_per_sm;
+    cfg.ctas_per_sm = c->ctas_per_sm;
     cfg.block_ns = ns;
     cfg.variant_start = c->ev[0];
     cfg.variant_stop = c->ev[1];
