@@ -291,6 +291,7 @@ def main():
 
     # Inputs resident in HBM for the device-timed value.
     d_entries = torch.from_numpy(entries.view(np.int64)).to(f"cuda:{local}")
+    torch.cuda.synchronize()
     stream = torch.cuda.Stream(device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
 

@@ -100,7 +100,9 @@ void tribit_default_options(tribit_options* opts);
 tribit_status tribit_create(const tribit_options* opts, tribit_context** ctx);
 void tribit_destroy(tribit_context* ctx);
 /* Run all later work of this context on `cuda_stream` (a cudaStream_t; NULL
- * restores the context's own stream). */
+ * restores the context's own stream). Waits for work queued on the previous
+ * stream. Device inputs given to later calls must be complete on the device
+ * when the call is made, or be produced on this stream. */
 tribit_status tribit_set_stream(tribit_context* ctx, void* cuda_stream);
 const char* tribit_status_string(tribit_status st);
 const char* tribit_last_error(const tribit_context* ctx);

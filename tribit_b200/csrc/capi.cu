@@ -214,8 +214,13 @@ void tribit_destroy(tribit_context* c) {
 
 tribit_status tribit_set_stream(tribit_context* c, void* stream) {
   if (!c) return TRIBIT_ERR_INVALID_ARGUMENT;
-  c->st = stream ? (cudaStream_t)stream : c->own;
-  return TRIBIT_OK;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    // Work already queued on the old stream finishes before any later call
+    // queues work on the new one (they share the context's buffers).
+    if (c->st) TB_CUDA(cudaStreamSynchronize(c->st));
+    c->st = stream ? (cudaStream_t)stream : c->own;
+  });
 }
 
 tribit_status tribit_count_edges(tribit_context* c, const uint64_t* entries, uint64_t n_entries, uint64_t num_nodes,

@@ -28,7 +28,10 @@ constexpr uint32_t kGrab = 4;                        // pieces taken per cursor 
 constexpr uint64_t kEmptySlot = 0xFFFFFFFF00000000ull;
 
 enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6 };
-constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 2;  // CTA-shared table in the same 32 KiB
+// Heavy phase: CTA-shared table in the first 16 KiB of the kernel's shared
+// memory, the row's per-neighbour item prefix in the second 16 KiB.
+constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 4;
+constexpr uint32_t kHeavyMaxDeg = kWarpsPerCta * kWarpSlots - 1;
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 enum { kOvfCta = 0, kOvfGlobal = 1 };
 constexpr int kTileMaxK = 64;  // bit-tile variant: at most this many column blocks (2048 columns)
@@ -260,6 +263,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
   // warps sweeping the row's neighbour chunks.
   if (heavy) {
     uint64_t* ctbl = &smem[0][0];
+    uint32_t* pre = reinterpret_cast<uint32_t*>(&smem[kWarpsPerCta / 2][0]);
     const uint32_t hlen = piece_off[TRIBIT_NUM_VARIANTS + 1];
     for (;;) {
       if (threadIdx.x == 0) {
@@ -271,18 +275,53 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       if (u == kNoRow) break;
       const uint64_t a = g.rp[u], b = g.rp[u + 1];
       const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
-      if (nb > kHeavyMaxBlocks) {
+      const uint32_t d = re - rs;
+      if (nb > kHeavyMaxBlocks || d > kHeavyMaxDeg) {
         if (threadIdx.x == 0) push_row(stats, kOvfCta, ovf_cta, u);
         __syncthreads();
         continue;
       }
       const int logb = table_logb(nb);
       table_clear(ctbl, logb, threadIdx.x, blockDim.x);
+      // Item prefix: pre[j] = bit blocks of the neighbours before j, pre[d] = all.
+      for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
+        const uint32_t v = g.col[rs + j];
+        pre[j] = rp_blk(g.rp[v + 1]) - rp_blk(g.rp[v]);
+      }
       __syncthreads();
       table_insert(ctbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
+      {
+        const uint32_t per = (d + blockDim.x - 1) / blockDim.x, j0 = threadIdx.x * per;
+        uint32_t lsum = 0;
+        for (uint32_t k = 0; k < per && j0 + k < d; ++k) lsum += pre[j0 + k];
+        uint32_t tot;
+        uint32_t ex = block_exclusive_scan<uint32_t>(lsum, OpSum{}, 0u, &tot);
+        for (uint32_t k = 0; k < per && j0 + k < d; ++k) {
+          const uint32_t x = pre[j0 + k];
+          pre[j0 + k] = ex;
+          ex += x;
+        }
+        if (threadIdx.x == 0) pre[d] = tot;
+      }
       __syncthreads();
+      // Warp w takes the neighbours whose first item falls in the w-th equal
+      // share of the row's items, so the warps finish together.
+      const uint32_t tot = pre[d];
+      auto first_at = [&](uint32_t x) -> uint32_t {  // first j with pre[j] >= x
+        uint32_t lo = 0, hi = d;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (pre[mid] < x)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        return lo;
+      };
+      const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kWarpsPerCta));
+      const uint32_t ce = w + 1 == kWarpsPerCta ? d : first_at((uint32_t)((uint64_t)tot * (w + 1) / kWarpsPerCta));
       const BitmapProbe probe{ctbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
-      const uint64_t racc = sweep<true>(g, rs, re, w, kWarpsPerCta,
+      const uint64_t racc = sweep<true>(g, rs + cs, rs + ce, 0, 1,
                                         [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
       if (per_graph) {
         const uint64_t s = warp_sum(racc);

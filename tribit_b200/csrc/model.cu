@@ -300,12 +300,13 @@ void require_model(tribit_context* c) {
 
 }  // namespace
 
-void model_alloc(DeviceModel& m) {
+void model_alloc(DeviceModel& m, cudaStream_t st) {
   if (m.master) return;
   float* base = nullptr;
   const size_t n = 5 * (size_t)kNumParams + kNorm;
   TB_CUDA(cudaMalloc(&base, n * sizeof(float)));
-  TB_CUDA(cudaMemset(base, 0, n * sizeof(float)));
+  // On the caller's stream: the uploads that follow are ordered after it.
+  TB_CUDA(cudaMemsetAsync(base, 0, n * sizeof(float), st));
   m.master = base;
   m.eff = base + kNumParams;
   m.m = base + 2 * kNumParams;
@@ -360,7 +361,7 @@ tribit_status tribit_model_init(tribit_context* c, uint64_t seed, const float* n
   if (!c || !norm) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     DeviceGuard dg(c->device);
-    tb::model_alloc(c->model);
+    tb::model_alloc(c->model, c->st);
     std::vector<float> p(tb::kNumParams, 0.f);
     auto fill = [&](int off, int fan_in, int count) {
       const double lim = std::sqrt(6.0 / fan_in);
@@ -565,7 +566,7 @@ tribit_status tribit_model_load(tribit_context* c, const char* path) {
     std::fclose(f);
     if (!ok) throw StatusError(TRIBIT_ERR_FORMAT, "not a tribit dispatcher model file");
     DeviceGuard dg(c->device);
-    tb::model_alloc(c->model);
+    tb::model_alloc(c->model, c->st);
     TB_CUDA(cudaMemcpyAsync(c->model.master, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice, c->st));
     TB_CUDA(cudaMemcpyAsync(c->model.norm, nrm.data(), nrm.size() * sizeof(float), cudaMemcpyHostToDevice, c->st));
     TB_CUDA(cudaMemsetAsync(c->model.m, 0, 2 * tb::kNumParams * sizeof(float), c->st));

@@ -33,7 +33,7 @@ struct DeviceModel {
   bool loaded = false;
 };
 
-void model_alloc(DeviceModel& m);
+void model_alloc(DeviceModel& m, cudaStream_t st);
 void model_free(DeviceModel& m);
 void model_refresh_eff(DeviceModel& m, cudaStream_t st);
 
