@@ -62,6 +62,20 @@ def make_graph(tb, spec, rank):
     raise ValueError(s["gen"])
 
 
+def reduce_replicas(dist, edges, seconds, device):
+    """Replicas only (no data-path collective): each rank counts its own graph.
+    Returns (edges summed over ranks, time maxed over ranks); with dist None,
+    this rank's own. The two reductions are the only collectives of the bench."""
+    if dist is None:
+        return edges, seconds
+    import torch
+    e = torch.tensor([edges], device=device, dtype=torch.float64)
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return int(e.item()), float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -334,14 +348,16 @@ def main():
             c.close()
     clk = clocks.summary()
     prep, res, ms = results[dispatch]
-    total_ms = sum(ms)
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
     m = res.edges
-    value = world * m / (ms_per_step / 1e3)
+    device = f"cuda:{local}"
+    # Whole job: every replica's edges over the slowest replica's time.
+    job_edges, total_ms = reduce_replicas(dist, m, sum(ms), device)
+    ms_per_step = total_ms / args.steps
+    value = job_edges / (ms_per_step / 1e3)
+    per_mode = {}
+    for k, v in results.items():
+        e_k, t_k = reduce_replicas(dist, v[1].edges, sum(v[2]), device)
+        per_mode[k] = e_k / (t_k / len(v[2]) / 1e3)
 
     # End to end through the public C-ABI call with pinned host entries.
     pinned = torch.empty(entries.size, dtype=torch.int64, pin_memory=True)
@@ -360,11 +376,7 @@ def main():
         e2e_s.append(time.perf_counter() - t1)
     c.close()
     assert e2e_res.triangles == res.triangles
-    e2e_t = statistics.mean(e2e_s)
-    if dist:
-        t = torch.tensor([e2e_t], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    _, e2e_t = reduce_replicas(dist, m, statistics.mean(e2e_s), device)
 
     peak, peak_kind = measured_peaks()
     b_alg = 4 * (n + 1) + 4 * m
@@ -393,15 +405,14 @@ def main():
                        "l2": "256 MiB buffer written between timed steps; inputs > L2",
                        "preprocess_ms": prep.preprocess_ms, "gen_s": round(gen_s, 2),
                        "row_blocks_by_variant": dict(zip(tb.VARIANTS, res.row_blocks_by_variant)),
-                       "per_mode_edges_per_s": {k: world * v[1].edges / (sum(v[2]) / len(v[2]) / 1e3)
-                                                for k, v in results.items()},
+                       "per_mode_edges_per_s": per_mode,
                        "batch": batch},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "algorithmic_bytes": b_alg},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * m / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
+            "e2e": {"value": job_edges / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
                     "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3},
             "clocks": clk,
             "gpu_launches": args.steps * res.count_kernels,

@@ -90,7 +90,8 @@ typedef struct tribit_result {
   float kernel_ms;            /* counting kernel(s) */
   float total_ms;             /* whole call, device time */
   uint32_t count_kernels;     /* kernels one counting launch issues */
-  uint32_t reserved;
+  uint32_t hub_edges;         /* edges the merge variant counts by walking u's tail against the
+                                 staged row of v (the hub pass) */
 } tribit_result;
 
 typedef struct tribit_context tribit_context;

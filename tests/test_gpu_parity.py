@@ -125,6 +125,31 @@ def test_big_rows_take_cta_and_global_paths():
                 assert c.count_edges(e, k + 1).triangles == comb(k + 1)
 
 
+def test_hub_pass_takes_short_tails_and_stays_exact():
+    # Power-law graphs: in merge row blocks, edges into high-rank hubs whose
+    # bit rows are longer than u's tail go to the hub pass; the rest stay with
+    # their rows. Every split must give the oracle's count.
+    for scale, seed in ((12, 1), (15, 2), (17, 3)):
+        n = 1 << scale
+        e = tb.gen_rmat(scale, 16, seed=seed)
+        want, m = oracle.count(e, n)
+        with tb.Counter(dispatch="merge") as c:
+            r = c.count_edges(e, n)
+            assert (r.triangles, r.edges) == (want, m)
+            assert 0 < r.hub_edges < m
+        with tb.Counter(dispatch="bitmap") as c:
+            r = c.count_edges(e, n)
+            assert r.triangles == want and r.hub_edges == 0
+    # A clique on top of a star: every rim vertex's tail is shorter than the
+    # rows of the higher-ranked clique members it points to.
+    k = 300
+    e = np.concatenate([clique(k, base=1), star(k + 1)])
+    for order in ("degree", "id"):
+        with tb.Counter(order=order, dispatch="merge") as c:
+            r = c.count_edges(e, k + 1)
+            assert r.triangles == comb(k + 1)
+
+
 def test_repeated_and_resized_calls(counters):
     c = counters[("degree", "plain")]
     cases = [generate(x["params"]) + (x,) for x in GENERATED[:4]]

@@ -52,7 +52,7 @@ class _Result(ctypes.Structure):
     _fields_ = [("triangles", _u64), ("num_nodes", _u64), ("entries", _u64), ("edges", _u64),
                 ("blocks_of_threads", _u64), ("row_blocks", _u64), ("row_blocks_by_variant", _u64 * 3),
                 ("h2d_ms", ctypes.c_float), ("preprocess_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
-                ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("reserved", _u32)]
+                ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("hub_edges", _u32)]
 
 
 def _decl(name, res, *args):
@@ -144,12 +144,13 @@ class Result:
     kernel_ms: float
     total_ms: float
     count_kernels: int
+    hub_edges: int
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         return cls(r.triangles, r.num_nodes, r.entries, r.edges, r.blocks_of_threads, r.row_blocks,
                    tuple(r.row_blocks_by_variant), r.h2d_ms, r.preprocess_ms, r.kernel_ms, r.total_ms,
-                   r.count_kernels)
+                   r.count_kernels, r.hub_edges)
 
 
 def _entries(a) -> np.ndarray:

@@ -115,9 +115,12 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
 }
 
 void fill_schedule_stats(tribit_context* c, tribit_result* res) {
-  uint32_t lens[TRIBIT_NUM_VARIANTS];
+  uint32_t lens[TRIBIT_NUM_VARIANTS], hub_edges = 0;
   TB_CUDA(cudaMemcpyAsync(lens, c->sched.list_len, sizeof lens, cudaMemcpyDeviceToHost, c->st));
+  TB_CUDA(cudaMemcpyAsync(&hub_edges, c->sched.piece_off + TRIBIT_NUM_VARIANTS + 3, sizeof hub_edges,
+                          cudaMemcpyDeviceToHost, c->st));
   TB_CUDA(cudaStreamSynchronize(c->st));
+  res->hub_edges = hub_edges;
   res->row_blocks = 0;
   for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) {
     res->row_blocks_by_variant[v] = lens[v];

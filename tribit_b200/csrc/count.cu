@@ -27,7 +27,7 @@ constexpr uint32_t kLong = 24;                       // lists at least this long
 constexpr uint32_t kGrab = 4;                        // pieces taken per cursor update
 constexpr uint64_t kEmptySlot = 0xFFFFFFFF00000000ull;
 
-enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6 };
+enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6, kCurHub = 7 };
 // Heavy phase: CTA-shared table in the first 16 KiB of the kernel's shared
 // memory, the row's per-neighbour item prefix in the second 16 KiB.
 constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 4;
@@ -93,45 +93,43 @@ struct BitmapProbe {
 };
 
 // ---- the neighbour sweep ---------------------------------------------------
-// For neighbours N+(u)[c] with c in [cs, ce) in chunks of 32 (chunk0,
-// chunk0 + step, ...) visits every item of each neighbour's list: its bit
-// blocks (Blocks) or its neighbour ids. item(k, c) returns the matches of item
-// index k of neighbour slot c. Must be called by all 32 lanes of the warp.
+// Visits every item of the lists of slots [cs, ce), in chunks of 32 slots
+// (chunk0, chunk0 + step, ...). desc(j, ib, il) gives slot j's first item and
+// item count (il = 0 skips it); item(k, j) returns the matches of item k of
+// slot j. Long lists are swept by all 32 lanes, two items per lane in flight;
+// short lists are flattened across lanes. Must be called by all 32 lanes.
 
-template <bool Blocks, class Item>
-__device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
-                                          uint32_t step, const Item& item) {
+template <class Desc, class Item>
+__device__ __forceinline__ uint64_t sweep_lists(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
+                                                const Desc& desc, const Item& item) {
   const uint32_t lane = threadIdx.x & 31;
   uint64_t acc = 0;
   for (uint32_t c = cs + chunk0 * 32; c < ce; c += step * 32) {
     const uint32_t j = c + lane;
     uint32_t ib = 0, il = 0;
-    if (j < ce) {
-      const uint32_t v = g.col[j];
-      const uint64_t a = g.rp[v], b = g.rp[v + 1];
-      ib = Blocks ? rp_blk(a) : rp_row(a);
-      il = (Blocks ? rp_blk(b) : rp_row(b)) - ib;
-    }
-    // Long lists: one neighbour at a time, all lanes, two items per lane in flight.
+    if (j < ce) desc(j, ib, il);
     uint32_t longm = __ballot_sync(kFull, il >= kLong);
     while (longm) {
       const int s = __ffs(longm) - 1;
       longm &= longm - 1;
       const uint32_t sb = __shfl_sync(kFull, ib, s), sl = __shfl_sync(kFull, il, s);
       const uint32_t cj = c + s;
+      uint32_t racc = 0;
       for (uint32_t k = lane; k < sl; k += 64) {
         const uint32_t k2 = k + 32;
         const uint32_t r0 = item(sb + k, cj);
         const uint32_t r1 = k2 < sl ? item(sb + k2, cj) : 0u;
-        acc += r0 + r1;
+        racc += r0 + r1;
       }
+      acc += racc;
     }
-    // Short lists: flattened over lanes; the owner of item t is the lane
-    // whose inclusive prefix first exceeds t.
+    // Short lists: the owner of flattened item t is the lane whose inclusive
+    // prefix first exceeds t.
     const uint32_t sl = il >= kLong ? 0u : il;
     const uint32_t incl = warp_inclusive_sum(sl);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t excl = incl - sl;
+    uint32_t racc = 0;
     for (uint32_t base = 0; base < total; base += 32) {
       const uint32_t t = base + lane;
       uint32_t s = 0;
@@ -142,10 +140,34 @@ __device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint3
       }
       const uint32_t sb = __shfl_sync(kFull, ib, s);
       const uint32_t se = __shfl_sync(kFull, excl, s);
-      if (t < total) acc += item(sb + (t - se), c + s);
+      if (t < total) racc += item(sb + (t - se), c + s);
     }
+    acc += racc;
   }
   return acc;
+}
+
+// Edge j of the CSR is counted by the hub pass (see k_hub) instead of by its
+// row's sweep.
+__device__ __forceinline__ bool edge_to_hub(const GraphView& g, uint32_t j) {
+  return g.eflag && ((g.eflag[j >> 5] >> (j & 31)) & 1u);
+}
+
+// The neighbour sweep: slots are CSR positions j, each the list of v = col[j]:
+// its bit blocks (Blocks) or its neighbour ids.
+template <bool Blocks, class Item>
+__device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
+                                          uint32_t step, const Item& item) {
+  return sweep_lists(
+      cs, ce, chunk0, step,
+      [&](uint32_t j, uint32_t& ib, uint32_t& il) {
+        if (edge_to_hub(g, j)) return;
+        const uint32_t v = g.col[j];
+        const uint64_t a = g.rp[v], b = g.rp[v + 1];
+        ib = Blocks ? rp_blk(a) : rp_row(a);
+        il = (Blocks ? rp_blk(b) : rp_row(b)) - ib;
+      },
+      item);
 }
 
 // Mask of block x in the sorted bit row r[lo, end), or 0.
@@ -169,7 +191,9 @@ __device__ __forceinline__ uint32_t search_mask(const uint64_t* r, uint32_t lo, 
 // shared memory (urow, nbu entries, ascending block). For each neighbour v of
 // the chunk, the shorter of u's tail -- u's entries from v's block on, the
 // only ones that can meet N+(v) -- and v's bit row is walked, and every block
-// of it is binary-searched in the other list. Must be called by all 32 lanes.
+// of it is binary-searched in the other list. Edges given to the hub pass,
+// where u's tail was the shorter list, are skipped. Must be called by all 32
+// lanes.
 __device__ __forceinline__ uint64_t sweep_merge(const GraphView& g, const uint64_t* urow, uint32_t nbu, uint32_t cs,
                                                 uint32_t ce) {
   const uint32_t lane = threadIdx.x & 31;
@@ -183,7 +207,7 @@ __device__ __forceinline__ uint64_t sweep_merge(const GraphView& g, const uint64
   for (uint32_t c = cs; c < ce; c += 32) {
     const uint32_t j = c + lane;
     uint32_t ab = 0, len = 0, ob = 0, oe = 0, walk_u = 0;
-    if (j < ce) {
+    if (j < ce && !edge_to_hub(g, j)) {
       const uint32_t v = g.col[j];
       const uint64_t va = g.rp[v], vb = g.rp[v + 1];
       const uint32_t vbs = rp_blk(va), vbe = rp_blk(vb);
@@ -286,7 +310,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       // Item prefix: pre[j] = bit blocks of the neighbours before j, pre[d] = all.
       for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
         const uint32_t v = g.col[rs + j];
-        pre[j] = rp_blk(g.rp[v + 1]) - rp_blk(g.rp[v]);
+        pre[j] = edge_to_hub(g, rs + j) ? 0u : rp_blk(g.rp[v + 1]) - rp_blk(g.rp[v]);
       }
       __syncthreads();
       table_insert(ctbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
@@ -707,6 +731,120 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
+// ---- hub pass: the merge variant's walks of u's tail ------------------------
+// For an edge (u, v) of a merge row block, the sorted-list intersection walks
+// the shorter of u's tail (u's bit blocks from v's block on: the only ones
+// that can meet N+(v)) and v's bit row. Where the tail is shorter and v's row
+// spans at most kHubMaxSpan blocks, the schedule groups the edge under v (the
+// hub) and flags it so the row sweeps skip it. A CTA then stages v's bit row
+// once as a direct-mapped array of masks over its block span, and its warps
+// walk the tails of a piece of v's in-edges against it: per tail block one
+// shared-memory load, AND and popc, and no search. Every edge is counted
+// exactly once, here or by its row.
+
+constexpr int kHubWarps = 8;
+constexpr uint32_t kHubMaxSpan = 8192;  // blocks of v's row span: 32 KiB of masks
+constexpr uint32_t kHubPiece = 1024;    // in-edges per piece
+constexpr int kHubCtasPerSm = 5;
+
+__global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
+                                                        const uint32_t* __restrict__ piece_off,
+                                                        const uint32_t* __restrict__ in_off,
+                                                        const uint64_t* __restrict__ inl,
+                                                        const uint32_t* __restrict__ inrow, DeviceStats* stats,
+                                                        unsigned long long* per_graph,
+                                                        unsigned long long* block_ns) {
+  __shared__ uint32_t map[kHubMaxSpan];
+  __shared__ uint32_t pre[kHubPiece + 1];
+  __shared__ uint32_t s_t;
+  __shared__ unsigned long long s_dt;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t len = piece_off[TRIBIT_NUM_VARIANTS + 2];
+  uint64_t acc = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(&stats->cursor[kCurHub], 1u);
+    __syncthreads();
+    const uint32_t t = s_t;
+    if (t >= len) break;
+    const unsigned long long t_start = block_ns ? cycles() : 0ull;
+    // Largest hubs first: pieces are in ascending v.
+    const uint64_t pc = hub_pieces[len - 1 - t];
+    const uint32_t v = (uint32_t)(pc >> 32);
+    const uint32_t e0 = in_off[v] + (uint32_t)pc;
+    const uint32_t cnt = min(kHubPiece, in_off[v + 1] - e0);
+    const uint64_t a = g.rp[v], b = g.rp[v + 1];
+    const uint32_t bs = rp_blk(a), be = rp_blk(b);
+    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32);
+    const uint32_t span = (uint32_t)(g.bent[be - 1] >> 32) - bmin + 1;  // <= kHubMaxSpan by the schedule
+    for (uint32_t i = threadIdx.x; i < span; i += blockDim.x) map[i] = 0u;
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) pre[i] = (uint32_t)inl[e0 + i];
+    __syncthreads();
+    for (uint32_t k = bs + threadIdx.x; k < be; k += blockDim.x) {
+      const uint64_t e = g.bent[k];
+      map[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+    }
+    // Tail-length prefix: pre[i] = blocks of the tails before i, pre[cnt] = all.
+    {
+      const uint32_t per = (cnt + blockDim.x - 1) / blockDim.x, j0 = threadIdx.x * per;
+      uint32_t lsum = 0;
+      for (uint32_t k = 0; k < per && j0 + k < cnt; ++k) lsum += pre[j0 + k];
+      uint32_t tot;
+      uint32_t ex = block_exclusive_scan<uint32_t>(lsum, OpSum{}, 0u, &tot);
+      for (uint32_t k = 0; k < per && j0 + k < cnt; ++k) {
+        const uint32_t x = pre[j0 + k];
+        pre[j0 + k] = ex;
+        ex += x;
+      }
+      if (threadIdx.x == 0) pre[cnt] = tot;
+    }
+    __syncthreads();
+    // Warp w walks the tails whose first block falls in the w-th equal share.
+    const uint32_t tot = pre[cnt];
+    auto first_at = [&](uint32_t x) -> uint32_t {  // first i with pre[i] >= x
+      uint32_t lo = 0, hi = cnt;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pre[mid] < x)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      return lo;
+    };
+    const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kHubWarps));
+    const uint32_t ce = w + 1 == kHubWarps ? cnt : first_at((uint32_t)((uint64_t)tot * (w + 1) / kHubWarps));
+    const uint64_t racc = sweep_lists(
+        cs, ce, 0, 1,
+        [&](uint32_t i, uint32_t& ib, uint32_t& il) {
+          const uint64_t x = inl[e0 + i];
+          ib = (uint32_t)(x >> 32);
+          il = (uint32_t)x;
+        },
+        [&](uint32_t k, uint32_t) -> uint32_t {
+          const uint64_t e = g.bent[k];
+          const uint32_t o = (uint32_t)(e >> 32) - bmin;
+          return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
+        });
+    if (per_graph) {
+      const uint64_t s = warp_sum(racc);
+      if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
+    }
+    acc += racc;
+    __syncthreads();
+    if (block_ns) {
+      // The piece's cycles, shared among its in-edges' row blocks by tail length.
+      if (threadIdx.x == 0) s_dt = cycles() - t_start;
+      __syncthreads();
+      const double per_block = (double)s_dt / (double)max(tot, 1u);
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+        atomicAdd(&block_ns[inrow[e0 + i] >> 5], (unsigned long long)(per_block * (pre[i + 1] - pre[i]) + 0.5));
+      __syncthreads();
+    }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+}
+
 // ---- schedule ----------------------------------------------------------------
 
 // Row-block features (one warp per row block) and the plain dispatcher's
@@ -869,16 +1007,115 @@ __global__ void k_piece_scatter(GraphView g, uint32_t nrb, const uint8_t* __rest
   }
 }
 
+// ---- hub schedule -----------------------------------------------------------
+
+// vinfo[v] = (span << 32) | nb: v's bit-row length and the blocks it spans.
+__global__ void k_hub_vinfo(GraphView g, uint64_t* __restrict__ vinfo) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= g.n) return;
+  const uint64_t a = g.rp[v], b = g.rp[v + 1];
+  const uint32_t bs = rp_blk(a), be = rp_blk(b);
+  uint64_t x = 0;
+  if (be > bs) {
+    const uint32_t span = (uint32_t)(g.bent[be - 1] >> 32) - (uint32_t)(g.bent[bs] >> 32) + 1;
+    x = ((uint64_t)span << 32) | (be - bs);
+  }
+  vinfo[v] = x;
+}
+
+// One pass over the edges of the merge row blocks, one warp per row. For the
+// edge at CSR position j, u's tail is u's bit blocks from v's block on.
+// Mode 0: save[v] += the blocks a hub walk saves (v's row length - tail) over
+// the edges where the tail is shorter and v's span fits. Mode 1: flags those
+// edges whose hub saves at least its staging cost (span / 4 + nb stores) and
+// counts them per hub. Mode 2: appends each flagged edge's tail (first block,
+// length) and row to its hub's in-list.
+template <int Mode>
+__global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of, const uint64_t* __restrict__ vinfo,
+                            unsigned long long* __restrict__ save, uint32_t* __restrict__ eflag,
+                            uint32_t* __restrict__ in_cnt, const uint32_t* __restrict__ in_off,
+                            uint64_t* __restrict__ inl, uint32_t* __restrict__ inrow) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < g.n; u += nwarps) {
+    if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
+    const uint64_t a = g.rp[u], b = g.rp[u + 1];
+    const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), nbu = rp_blk(b) - bs;
+    if (re - rs < 2) continue;
+    uint32_t carry = 0, prev_last = 0xFFFFFFFFu;
+    for (uint32_t c = rs; c < re; c += 32) {
+      const uint32_t j = c + lane;
+      const bool in = j < re;
+      const uint32_t v = in ? g.col[j] : 0u;
+      const uint32_t blk = in ? v >> 5 : 0xFFFFFFFFu;
+      uint32_t prev = __shfl_up_sync(kFull, blk, 1);
+      if (lane == 0) prev = prev_last;
+      const uint32_t incl = warp_inclusive_sum((in && blk != prev) ? 1u : 0u);
+      const uint32_t pos = carry + incl - 1;  // index of v's block in u's bit row
+      carry += __shfl_sync(kFull, incl, 31);
+      prev_last = __shfl_sync(kFull, blk, 31);
+      const uint32_t tail = nbu - pos;
+      bool hub = false;
+      uint32_t nbv = 0, span = 0;
+      if (in) {
+        const uint64_t vi = vinfo[v];
+        nbv = (uint32_t)vi;
+        span = (uint32_t)(vi >> 32);
+        hub = nbv > 0 && span <= kHubMaxSpan && tail < nbv;
+      }
+      if (Mode == 0) {
+        if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
+      } else if (Mode == 1) {
+        hub = hub && save[v] >= (unsigned long long)(span / 4 + nbv);
+        const uint32_t bits = __ballot_sync(kFull, hub);
+        if (lane == 0 && bits) {
+          const uint32_t sh = c & 31;
+          atomicOr(&eflag[c >> 5], bits << sh);
+          if (sh && (bits >> (32 - sh))) atomicOr(&eflag[(c >> 5) + 1], bits >> (32 - sh));
+        }
+        if (hub) atomicAdd(&in_cnt[v], 1u);
+      } else {
+        if (in && ((eflag[j >> 5] >> (j & 31)) & 1u)) {
+          const uint32_t at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
+          inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
+          inrow[at] = u;
+        }
+      }
+    }
+  }
+}
+
+// Pieces per hub: ceil(in-edges / kHubPiece); cnt[n] = 0 for the scan.
+__global__ void k_hub_piece_count(const uint32_t* __restrict__ in_off, uint32_t n, uint32_t* __restrict__ cnt) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v > n) return;
+  cnt[v] = v < n ? (in_off[v + 1] - in_off[v] + kHubPiece - 1) / kHubPiece : 0u;
+}
+
+__global__ void k_hub_piece_scatter(const uint32_t* __restrict__ pos, uint32_t n, uint64_t* __restrict__ pieces,
+                                    uint32_t* __restrict__ piece_off) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n)
+    for (uint32_t k = 0, np = pos[v + 1] - pos[v]; k < np; ++k)
+      pieces[pos[v] + k] = ((uint64_t)v << 32) | (k * kHubPiece);
+  if (v == n) piece_off[TRIBIT_NUM_VARIANTS + 2] = pos[n];
+}
+
+__global__ void k_hub_total(const uint32_t* __restrict__ in_off, uint32_t n, uint32_t* __restrict__ piece_off) {
+  piece_off[TRIBIT_NUM_VARIANTS + 3] = in_off[n];
+}
+
 }  // namespace
 
-Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E) {
+Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
   Schedule s;
   const uint32_t nrb = (uint32_t)ceil_div<uint64_t>(n, 32);
   s.num_row_blocks = nrb;
   s.variant_of = ar.take<uint8_t>(nrb + 1);
   s.piece_cap = n + E / kMinPieceWidth + 64;
   s.pieces = ar.take<uint64_t>(s.piece_cap);
-  s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 2);
+  s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 4);
   s.heavy = ar.take<uint32_t>(n + 1);
   s.row_flags = ar.take<uint32_t>(n + 1);
   s.row_scan_tmp = take_scan_temp<uint32_t>(ar, n + 1);
@@ -889,7 +1126,54 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E) {
   s.overflow_cap = (uint32_t)(n + 1);
   s.overflow = ar.take<uint32_t>(2 * (n + 1));
   s.features = ar.take<float>((uint64_t)nrb * kNumFeatures + 1);
+  if (hubs) {
+    s.eflag_words = E / 32 + 2;
+    s.eflag = ar.take<uint32_t>(s.eflag_words);
+    s.vinfo = ar.take<uint64_t>(n + 1);
+    s.save = ar.take<unsigned long long>(n + 1);
+    s.in_cnt = ar.take<uint32_t>(n + 1);
+    s.in_off = ar.take<uint32_t>(n + 1);
+    s.inl = ar.take<uint64_t>(E + 1);
+    s.inrow = ar.take<uint32_t>(E + 1);
+    s.hub_pieces = ar.take<uint64_t>(n + E / kHubPiece + 64);
+  }
   return s;
+}
+
+// Hub in-lists and pieces of the merge row blocks (after the heavy-row list:
+// row_flags and its scan space are reused). Without hub arrays, or with
+// hubs off, the hub pass gets no pieces and no edge is flagged.
+static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
+  s.hubs_active = false;
+  TB_CUDA(cudaMemsetAsync(s.piece_off + TRIBIT_NUM_VARIANTS + 2, 0, 2 * sizeof(uint32_t), st));
+  if (!s.eflag || !s.hubs || g.n == 0) return;
+  const uint64_t n = g.n;
+  const unsigned vblocks = (unsigned)ceil_div<uint64_t>(n + 1, 256);
+  const unsigned eblocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(n, 8), 148ull * 16));
+  k_hub_vinfo<<<vblocks, 256, 0, st>>>(g, s.vinfo);
+  TB_LAUNCH_CHECK();
+  TB_CUDA(cudaMemsetAsync(s.save, 0, n * sizeof(unsigned long long), st));
+  TB_CUDA(cudaMemsetAsync(s.eflag, 0, (s.eflag_words) * sizeof(uint32_t), st));
+  TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
+  k_hub_edges<0><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                           s.inrow);
+  TB_LAUNCH_CHECK();
+  k_hub_edges<1><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                           s.inrow);
+  TB_LAUNCH_CHECK();
+  device_scan<uint32_t, OpSum>(s.in_cnt, s.in_off, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
+  TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
+  k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                           s.inrow);
+  TB_LAUNCH_CHECK();
+  k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, (uint32_t)n, s.row_flags);
+  TB_LAUNCH_CHECK();
+  device_scan<uint32_t, OpSum>(s.row_flags, s.row_flags, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
+  k_hub_piece_scatter<<<vblocks, 256, 0, st>>>(s.row_flags, (uint32_t)n, s.hub_pieces, s.piece_off);
+  TB_LAUNCH_CHECK();
+  k_hub_total<<<1, 1, 0, st>>>(s.in_off, (uint32_t)n, s.piece_off);
+  TB_LAUNCH_CHECK();
+  s.hubs_active = true;
 }
 
 void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
@@ -919,6 +1203,7 @@ void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
   device_scan<uint32_t, OpSum>(s.row_flags, s.row_flags, (uint64_t)g.n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
   k_heavy_scatter<<<rblocks, 256, 0, st>>>(g, s.row_flags, s.heavy, s.piece_off);
   TB_LAUNCH_CHECK();
+  build_hubs(g, s, st);
 }
 
 void compute_features(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st) {
@@ -935,8 +1220,10 @@ void build_schedule(const GraphView& g, Schedule& s, int mode, bool full_feature
   build_pieces(g, s, st);
 }
 
-LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stats, unsigned long long* per_graph,
+LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* stats, unsigned long long* per_graph,
                         const CountConfig& cfg, cudaStream_t st) {
+  GraphView g = graph;
+  g.eflag = s.hubs_active ? s.eflag : nullptr;
   static bool attr_done = false;
   if (!attr_done) {
     TB_CUDA(cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -977,9 +1264,12 @@ LaunchInfo launch_count(const GraphView& g, const Schedule& s, DeviceStats* stat
   TB_LAUNCH_CHECK();
   k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
   TB_LAUNCH_CHECK();
+  k_hub<<<(unsigned)(sms * kHubCtasPerSm), kHubWarps * 32, 0, st>>>(g, s.hub_pieces, s.piece_off, s.in_off, s.inl,
+                                                                     s.inrow, stats, per_graph, cfg.block_ns);
+  TB_LAUNCH_CHECK();
   if (cfg.variant_stop) TB_CUDA(cudaEventRecord(cfg.variant_stop, st));
-  info.ctas = 2ull * warp_grid + 7ull * sms;
-  info.kernels = 5;
+  info.ctas = 2ull * warp_grid + (7ull + kHubCtasPerSm) * sms;
+  info.kernels = 6;
   return info;
 }
 

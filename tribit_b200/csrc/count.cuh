@@ -29,7 +29,8 @@ struct Schedule {
   uint8_t* variant_of = nullptr;   // device, per row block
   uint64_t* pieces = nullptr;      // device, (row << 32) | first neighbour, grouped by variant
   uint64_t piece_cap = 0;
-  uint32_t* piece_off = nullptr;   // device, TRIBIT_NUM_VARIANTS + 1 segment starts, then the heavy-row count
+  uint32_t* piece_off = nullptr;   // device, TRIBIT_NUM_VARIANTS + 1 segment starts, the heavy-row count,
+                                   // the hub-piece count, the hub-edge count
   uint32_t* heavy = nullptr;       // device, rows too wide for one warp, counted CTA-cooperatively first
   uint32_t* row_flags = nullptr;   // device, n + 1 scratch for the heavy-row scan
   uint32_t* row_scan_tmp = nullptr;
@@ -40,6 +41,18 @@ struct Schedule {
   uint32_t* overflow = nullptr;    // device, rows deferred to the CTA / global passes
   uint32_t overflow_cap = 0;
   float* features = nullptr;       // device, nrb x kNumFeatures
+  // Hub pass of the merge variant (absent when taken without hubs).
+  uint32_t* eflag = nullptr;       // device, bit per CSR position: edge counted by the hub pass
+  uint64_t eflag_words = 0;
+  uint64_t* vinfo = nullptr;       // device, n: (row span in blocks << 32) | bit-row length
+  unsigned long long* save = nullptr;  // device, n: blocks a hub walk would save
+  uint32_t* in_cnt = nullptr;      // device, n + 1
+  uint32_t* in_off = nullptr;      // device, n + 1: in-list of hub v at [in_off[v], in_off[v+1])
+  uint64_t* inl = nullptr;         // device: (first block of u's tail << 32) | tail length
+  uint32_t* inrow = nullptr;       // device: u of each in-list entry
+  uint64_t* hub_pieces = nullptr;  // device: (v << 32) | first in-list entry
+  bool hubs = true;                // build the hub lists for merge row blocks
+  bool hubs_active = false;        // set by build_pieces
   uint32_t piece_width = 64;       // neighbours per piece (tuned)
   float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
   const void* model = nullptr;     // device MLP parameters for learned dispatch
@@ -54,7 +67,8 @@ struct CountConfig {
   cudaEvent_t variant_stop = nullptr;      // their own; these events bracket the variant kernels
 };
 
-Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E);
+// hubs: also take the hub-pass arrays (about 13 bytes per entry).
+Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs = true);
 
 // Computes row-block features, the per-block variant (mode: TRIBIT_DISPATCH_*),
 // and the per-variant piece lists. full_features adds the neighbour-side

@@ -336,6 +336,7 @@ void apply_dispatch(tribit_context* c, cudaStream_t st) {
   const int mode = c->opts.dispatch;
   c->sched.piece_width = c->piece_width;
   c->sched.tile_min_nnz = c->tile_min_nnz;
+  c->sched.hubs = mode == TRIBIT_DISPATCH_LEARNED || mode == TRIBIT_DISPATCH_MERGE;  // only merge blocks use them
   drop_graph(c);
   if (mode == TRIBIT_DISPATCH_LEARNED) {
     require_model(c);
@@ -510,6 +511,7 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     unsigned long long* ns = ar.take<unsigned long long>(nrb + 1);
     TB_CUDA(cudaMemsetAsync(ns, 0, (nrb + 1) * sizeof(unsigned long long), c->st));
     if (nrb) TB_CUDA(cudaMemsetAsync(c->sched.variant_of, variant, nrb, c->st));
+    c->sched.hubs = variant == TRIBIT_VARIANT_MERGE;
     tb::build_pieces(c->prep.view, c->sched, c->st);
     tb::CountConfig cfg;
     cfg.num_sms = c->num_sms;

@@ -99,13 +99,13 @@ extern "C" tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, u
     {
       tb::Prepared probe;
       tb::prepare_graph(ar, in, st, &probe);
-      (void)tb::take_schedule(ar, num_nodes, n_entries);
+      (void)tb::take_schedule(ar, num_nodes, n_entries, false);
     }
     ar.reserve(ar.used());
     ar.begin(false);
     tb::Prepared prep;
     tb::prepare_graph(ar, in, st, &prep);
-    tb::Schedule sched = tb::take_schedule(ar, num_nodes, n_entries);
+    tb::Schedule sched = tb::take_schedule(ar, num_nodes, n_entries, false);
     tb::build_schedule(prep.view, sched, TRIBIT_DISPATCH_PLAIN, false, st);
     tb::CountConfig cfg;
     cfg.num_sms = sms;

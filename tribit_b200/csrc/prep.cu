@@ -240,6 +240,7 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
   out->view.n = (uint32_t)n;
   out->view.rp = rp;
   out->view.graph_of_rank = graph_of_rank;
+  out->view.eflag = nullptr;
 
   // Phase 1 (launch only when not measuring): degrees and the rank order.
   if (!ar.measuring()) {

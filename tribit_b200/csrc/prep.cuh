@@ -25,6 +25,8 @@ struct GraphView {
                                   // at [brow_ptr[u], brow_ptr[u+1]); bit (w & 31) of
                                   // block w >> 5 is set iff w in N+(u)
   const uint32_t* graph_of_rank;  // batch mode: graph id of each rank, else null
+  const uint32_t* eflag;          // per CSR position, bit set: the edge is counted by the
+                                  // hub pass, not by its row (set by the schedule), or null
 };
 
 __device__ __forceinline__ uint32_t rp_row(uint64_t w) { return (uint32_t)(w >> 32); }
