@@ -147,6 +147,48 @@ __device__ __forceinline__ uint64_t sweep_lists(uint32_t cs, uint32_t ce, uint32
   return acc;
 }
 
+// Flattened sweep for latency-bound lists: the lists of each chunk of 32
+// slots are concatenated and lane l takes items t = base + l + 32 r, r <
+// Depth, of the concatenation; the owner slot of item t is found by a binary
+// search over the chunk's inclusive length prefix (shuffles). A lane issues
+// all Depth loads before it uses any, so a warp keeps 32 * Depth loads in
+// flight however long or short the lists are. load(k) reads item k (index
+// into the item array), probe(x) scores it; a loaded 0 must score 0.
+template <int Depth, class Desc, class Load, class Probe>
+__device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, const Desc& desc, const Load& load,
+                                               const Probe& probe) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t acc = 0;
+  for (uint32_t c = cs; c < ce; c += 32) {
+    const uint32_t j = c + lane;
+    uint32_t ib = 0, il = 0;
+    if (j < ce) desc(j, ib, il);
+    const uint32_t incl = warp_inclusive_sum(il);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t off = ib - (incl - il);  // item t of the chunk, owned by slot s, is item off_s + t
+    uint32_t racc = 0;
+    for (uint32_t base = 0; base < total; base += 32 * Depth) {
+      uint64_t x[Depth];
+#pragma unroll
+      for (int r = 0; r < Depth; ++r) {
+        const uint32_t t = base + 32 * r + lane;
+        uint32_t s = 0;
+#pragma unroll
+        for (uint32_t st = 16; st >= 1; st >>= 1) {
+          const uint32_t y = __shfl_sync(kFull, incl, s + st - 1);
+          if (y <= t) s += st;
+        }
+        const uint32_t o = __shfl_sync(kFull, off, s);
+        x[r] = t < total ? load(o + t) : 0ull;
+      }
+#pragma unroll
+      for (int r = 0; r < Depth; ++r) racc += probe(x[r]);
+    }
+    acc += racc;
+  }
+  return acc;
+}
+
 // Edge j of the CSR is counted by the hub pass (see k_hub) instead of by its
 // row's sweep.
 __device__ __forceinline__ bool edge_to_hub(const GraphView& g, uint32_t j) {
@@ -746,6 +788,7 @@ constexpr int kHubWarps = 8;
 constexpr uint32_t kHubMaxSpan = 8192;  // blocks of v's row span: 32 KiB of masks
 constexpr uint32_t kHubPiece = 1024;    // in-edges per piece
 constexpr int kHubCtasPerSm = 5;
+constexpr int kHubDepth = 4;            // tail blocks in flight per lane
 
 __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
@@ -813,15 +856,15 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     };
     const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kHubWarps));
     const uint32_t ce = w + 1 == kHubWarps ? cnt : first_at((uint32_t)((uint64_t)tot * (w + 1) / kHubWarps));
-    const uint64_t racc = sweep_lists(
-        cs, ce, 0, 1,
+    const uint64_t racc = sweep_flat<kHubDepth>(
+        cs, ce,
         [&](uint32_t i, uint32_t& ib, uint32_t& il) {
           const uint64_t x = inl[e0 + i];
           ib = (uint32_t)(x >> 32);
           il = (uint32_t)x;
         },
-        [&](uint32_t k, uint32_t) -> uint32_t {
-          const uint64_t e = g.bent[k];
+        [&](uint32_t k) -> uint64_t { return g.bent[k]; },
+        [&](uint64_t e) -> uint32_t {
           const uint32_t o = (uint32_t)(e >> 32) - bmin;
           return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
         });
