@@ -784,11 +784,18 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 // shared-memory load, AND and popc, and no search. Every edge is counted
 // exactly once, here or by its row.
 
+// Build-time tunables (-D...): measured defaults.
+#ifndef TB_HUB_PIECE
+#define TB_HUB_PIECE 1024
+#endif
+#ifndef TB_HUB_DEPTH
+#define TB_HUB_DEPTH 8
+#endif
 constexpr int kHubWarps = 8;
-constexpr uint32_t kHubMaxSpan = 8192;  // blocks of v's row span: 32 KiB of masks
-constexpr uint32_t kHubPiece = 1024;    // in-edges per piece
+constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
+constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per piece
 constexpr int kHubCtasPerSm = 5;
-constexpr int kHubDepth = 4;            // tail blocks in flight per lane
+constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lane
 
 __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
