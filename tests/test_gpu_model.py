@@ -87,6 +87,28 @@ def test_learned_dispatch_counts_exactly():
                 assert c.count_edges(e, n).triangles == oracle.count(e, n)[0]
 
 
+def test_learned_dispatch_keeps_bit_tiles_to_blocks_that_fit_one_tile():
+    # A network that rates bit tiles cheapest everywhere may still only send
+    # the row blocks whose columns span 1..64 blocks to them.
+    import torch
+    e = tb.gen_rmat(15, 16, seed=43)
+    n = 1 << 15
+    d = torch.from_numpy(e.view(np.int64)).cuda()
+    with tb.Counter(dispatch="learned") as c:
+        norm = np.concatenate([np.zeros(16), np.ones(16), np.zeros(3), np.ones(3)]).astype(np.float32)
+        c.model_init(norm, seed=1)
+        p = c.model_params()
+        p[5440:5443] = [-1e4, 0.0, 1e4]  # predicted: MMA cheapest, then bitmap
+        c.set_model_params(p)
+        r = c.prepare_device(d.data_ptr(), d.numel(), n)
+        span = np.exp2(c.block_features()[:, 13]) - 1
+        eligible = int(((span > 0.5) & (span <= 64.5)).sum())
+        mma, bitmap, merge = r.row_blocks_by_variant
+        assert 0 < mma <= eligible and merge == 0 and bitmap > 0
+        c.launch_count()
+        assert c.read_count().triangles == oracle.count(e, n)[0]
+
+
 def test_block_features_and_times():
     import torch
     e = tb.gen_rmat(16, 16, seed=9)

@@ -34,7 +34,6 @@ constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 4;
 constexpr uint32_t kHeavyMaxDeg = kWarpsPerCta * kWarpSlots - 1;
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 enum { kOvfCta = 0, kOvfGlobal = 1 };
-constexpr int kTileMaxK = 64;  // bit-tile variant: at most this many column blocks (2048 columns)
 
 __device__ __forceinline__ int log2_ceil(uint32_t x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
 
@@ -155,11 +154,11 @@ __device__ __forceinline__ uint64_t sweep_lists(uint32_t cs, uint32_t ce, uint32
 // flight however long or short the lists are. load(k) reads item k (index
 // into the item array), probe(x) scores it; a loaded 0 must score 0.
 template <int Depth, class Desc, class Load, class Probe>
-__device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, const Desc& desc, const Load& load,
-                                               const Probe& probe) {
+__device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
+                                               const Desc& desc, const Load& load, const Probe& probe) {
   const uint32_t lane = threadIdx.x & 31;
   uint64_t acc = 0;
-  for (uint32_t c = cs; c < ce; c += 32) {
+  for (uint32_t c = cs + chunk0 * 32; c < ce; c += step * 32) {
     const uint32_t j = c + lane;
     uint32_t ib = 0, il = 0;
     if (j < ce) desc(j, ib, il);
@@ -210,6 +209,31 @@ __device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint3
         il = (Blocks ? rp_blk(b) : rp_row(b)) - ib;
       },
       item);
+}
+
+// Bit-row sweep: every bit block of v = col[j], j in the slots, scored by
+// probe (a hash or direct-map lookup in u's staged row). Flattened with
+// kBitsDepth blocks in flight per lane (see sweep_flat).
+#ifndef TB_BITS_DEPTH
+#define TB_BITS_DEPTH 4
+#endif
+constexpr int kBitsDepth = TB_BITS_DEPTH;
+
+template <class Probe>
+__device__ __forceinline__ uint64_t sweep_bits(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
+                                               uint32_t step, const Probe& probe) {
+  if (kBitsDepth == 0)
+    return sweep<true>(g, cs, ce, chunk0, step, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+  return sweep_flat<kBitsDepth == 0 ? 1 : kBitsDepth>(
+      cs, ce, chunk0, step,
+      [&](uint32_t j, uint32_t& ib, uint32_t& il) {
+        if (edge_to_hub(g, j)) return;
+        const uint32_t v = g.col[j];
+        const uint64_t a = g.rp[v], b = g.rp[v + 1];
+        ib = rp_blk(a);
+        il = rp_blk(b) - ib;
+      },
+      [&](uint32_t k) -> uint64_t { return g.bent[k]; }, probe);
 }
 
 // Mask of block x in the sorted bit row r[lo, end), or 0.
@@ -316,7 +340,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
                                                                     unsigned long long* per_graph,
                                                                     unsigned long long* block_ns,
                                                                     const uint32_t* __restrict__ heavy,
-                                                                    int do_pieces, uint32_t width) {
+                                                                    uint32_t width) {
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
   __shared__ uint32_t s_row;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -339,6 +363,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       __syncthreads();
       const uint32_t u = s_row;
       if (u == kNoRow) break;
+      const unsigned long long h_start = (block_ns && threadIdx.x == 0) ? cycles() : 0ull;
       const uint64_t a = g.rp[u], b = g.rp[u + 1];
       const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
       const uint32_t d = re - rs;
@@ -387,21 +412,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kWarpsPerCta));
       const uint32_t ce = w + 1 == kWarpsPerCta ? d : first_at((uint32_t)((uint64_t)tot * (w + 1) / kWarpsPerCta));
       const BitmapProbe probe{ctbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
-      const uint64_t racc = sweep<true>(g, rs + cs, rs + ce, 0, 1,
-                                        [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+      const uint64_t racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe);
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
         if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
       }
       acc += racc;
       __syncthreads();  // the table and s_row are rewritten for the next row
+      // Timing: the row's CTA cycles in warp-cycles, like the warp pieces'.
+      if (block_ns && threadIdx.x == 0) atomicAdd(&block_ns[u >> 5], (cycles() - h_start) * kWarpsPerCta);
     }
     __syncthreads();
-  }
-  if (!do_pieces) {
-    acc = warp_sum(acc);
-    if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
-    return;
   }
   uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
   bool cur_ok = false;
@@ -454,7 +475,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         racc = sweep_merge(g, tbl, d, cs, ce);
       } else {
         const BitmapProbe probe{tbl, logb, bmin, bmax};
-        racc = sweep<true>(g, cs, ce, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+        racc = sweep_bits(g, cs, ce, 0, 1, probe);
       }
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
@@ -517,7 +538,7 @@ __device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl
     __syncwarp();
     const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
     const uint64_t racc =
-        sweep<true>(g, rs, re, 0, 1, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+        sweep_bits(g, rs, re, 0, 1, probe);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
@@ -723,11 +744,11 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_cta(GraphView g, const uin
     __syncthreads();
     const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
     const uint64_t racc =
-        sweep<true>(g, rs, re, w, nw, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
+        sweep_bits(g, rs, re, w, nw, probe);
     const uint64_t s = block_sum_u64(racc);  // also the barrier before the table is rebuilt
     if (threadIdx.x == 0) {
       if (per_graph && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
-      if (block_ns) atomicAdd(&block_ns[u >> 5], cycles() - t_start);
+      if (block_ns) atomicAdd(&block_ns[u >> 5], (cycles() - t_start) * (blockDim.x >> 5));
     }
     acc += racc;
   }
@@ -864,7 +885,7 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kHubWarps));
     const uint32_t ce = w + 1 == kHubWarps ? cnt : first_at((uint32_t)((uint64_t)tot * (w + 1) / kHubWarps));
     const uint64_t racc = sweep_flat<kHubDepth>(
-        cs, ce,
+        cs, ce, 0, 1,
         [&](uint32_t i, uint32_t& ib, uint32_t& il) {
           const uint64_t x = inl[e0 + i];
           ib = (uint32_t)(x >> 32);
@@ -882,10 +903,10 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     acc += racc;
     __syncthreads();
     if (block_ns) {
-      // The piece's cycles, shared among its in-edges' row blocks by tail length.
+      // The piece's warp-cycles, shared among its in-edges' row blocks by tail length.
       if (threadIdx.x == 0) s_dt = cycles() - t_start;
       __syncthreads();
-      const double per_block = (double)s_dt / (double)max(tot, 1u);
+      const double per_block = (double)s_dt * kHubWarps / (double)max(tot, 1u);  // warp-cycles per tail block
       for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
         atomicAdd(&block_ns[inrow[e0 + i] >> 5], (unsigned long long)(per_block * (pre[i + 1] - pre[i]) + 0.5));
       __syncthreads();
@@ -1290,23 +1311,17 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
   TB_CUDA(cudaMemsetAsync(&stats->triangles, 0, sizeof(stats->triangles), st));
   uint32_t* ovf_cta = s.overflow;
   uint32_t* ovf_global = s.overflow + s.overflow_cap;
-  if (cfg.variant_start) {
-    // Timing mode: the heavy rows (the same for every variant) run first, on
-    // their own, so the events bracket only the variant kernels.
-    k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-        g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, nullptr, s.heavy, 0, s.piece_width);
-    TB_LAUNCH_CHECK();
-    TB_CUDA(cudaEventRecord(cfg.variant_start, st));
-  }
+  // Timing mode: the events bracket every counting kernel, and every piece,
+  // heavy row, tile block and hub piece adds its warp-cycles to its row block.
+  if (cfg.variant_start) TB_CUDA(cudaEventRecord(cfg.variant_start, st));
   k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
-      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, cfg.variant_start ? nullptr : s.heavy, 1,
-      s.piece_width);
+      g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy, s.piece_width);
   TB_LAUNCH_CHECK();
   k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
       g, s.variant_of, s.num_row_blocks, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
-                                                                               per_graph, cfg.block_ns, nullptr, 1,
+                                                                               per_graph, cfg.block_ns, nullptr,
                                                                                s.piece_width);
   TB_LAUNCH_CHECK();
   k_rows_cta<<<(unsigned)sms, kCtaThreads, sizeof(uint64_t) << kCtaLogSlots, st>>>(g, ovf_cta, stats, ovf_global,

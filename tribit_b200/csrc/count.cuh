@@ -22,6 +22,8 @@
 namespace tb {
 
 constexpr int kNumFeatures = 16;
+constexpr int kTileMaxK = 64;  // bit-tile variant: row blocks spanning at most this many column blocks
+constexpr int kFeatSpan = 13;  // feature index of log2(1 + column-block span)
 constexpr uint32_t kMinPieceWidth = 32;  // piece_width is a multiple of 32, at least this
 
 struct Schedule {
@@ -62,9 +64,9 @@ struct Schedule {
 struct CountConfig {
   int ctas_per_sm = 0;  // 0 = default
   int num_sms = 148;
-  unsigned long long* block_ns = nullptr;  // optional: per-row-block SM cycles, summed over pieces
-  cudaEvent_t variant_start = nullptr;     // optional (timing mode): heavy rows run first, on
-  cudaEvent_t variant_stop = nullptr;      // their own; these events bracket the variant kernels
+  unsigned long long* block_ns = nullptr;  // optional: per-row-block warp-cycles (SM cycles x warps busy)
+  cudaEvent_t variant_start = nullptr;     // optional (timing mode): these events bracket
+  cudaEvent_t variant_stop = nullptr;      // all counting kernels
 };
 
 // hubs: also take the hub-pass arrays (about 13 bytes per entry).

@@ -232,11 +232,17 @@ __global__ void __launch_bounds__(kModelThreads) k_dispatch(const float* __restr
     float out[kOut];
     row_pass<false>(s, feat + (size_t)rb * kIn, nullptr, 0.f, out, nullptr, 0, nullptr);
     if ((threadIdx.x & 31) == 0) {
-      int best = 0;
-      float bt = out[0] * s.norm[2 * kIn + kOut] + s.norm[2 * kIn];
-      for (int o = 1; o < kOut; ++o) {
+      // Bit tiles only where the block fits one tile (span of 1..kTileMaxK
+      // column blocks); elsewhere the tile kernel would sweep the block's rows
+      // one at a time on a single warp.
+      const float span = feat[(size_t)rb * kIn + kFeatSpan];
+      const bool tile_ok = span > 0.f && span <= log2f(1.f + (float)kTileMaxK) + 1e-4f;
+      int best = -1;
+      float bt = 0.f;
+      for (int o = 0; o < kOut; ++o) {
+        if (o == TRIBIT_VARIANT_MMA && !tile_ok) continue;
         const float t = out[o] * s.norm[2 * kIn + kOut + o] + s.norm[2 * kIn + o];
-        if (t < bt) bt = t, best = o;
+        if (best < 0 || t < bt) bt = t, best = o;
       }
       variant_of[rb] = (uint8_t)best;
     }

@@ -103,6 +103,15 @@ def plain_choice(x):
     return choice
 
 
+def learned_choice(pred, x):
+    """The learned dispatcher's rule (k_dispatch): the variant of least predicted
+    cost, bit tiles only for blocks that fit one tile (span of 1..64 blocks)."""
+    span = np.exp2(x[:, 13]) - 1
+    p = pred.copy()
+    p[~((span > 0.5) & (span <= 64.5)), tb.VARIANTS.index("mma")] = np.inf
+    return p.argmin(1)
+
+
 def timed_count(n, e, dispatch, model, steps=5):
     import torch
     d = torch.from_numpy(e.view(np.int64)).cuda()
@@ -156,7 +165,7 @@ def main():
         os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
         c.save_model(args.out)
         pred = c.model_predict(hx)
-    learned = pred.argmin(1)
+    learned = learned_choice(pred, hx)
     plain = plain_choice(hx)
     rows = np.arange(ht.shape[0])
     best = ht.min(1).sum()
