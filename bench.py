@@ -211,6 +211,7 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     c1 = tb.Counter(device=local, dispatch=dispatch)
     if dispatch == "learned":
         c1.load_model(model_path)
+    c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz)  # the batch's tuned settings
     idx = np.linspace(0, num_graphs - 1, per_graph_sample).astype(int)
     k_ms, e2e_one = 0.0, 0.0
     for g in idx:
@@ -231,6 +232,7 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
         "e2e_graphs_per_s_batched": num_graphs / e2e_s,
         "e2e_graphs_per_s_per_graph": num_graphs / (e2e_one * scale),
         "per_graph_sample": per_graph_sample, "tuning": tune.as_dict(), "cuda_graph": True,
+        "row_blocks_by_variant": dict(zip(tb.VARIANTS, r.row_blocks_by_variant)),
     }
 
 

@@ -128,7 +128,8 @@ tribit_status tribit_read_count(tribit_context* ctx, tribit_result* out);
 typedef struct tribit_tuning {
   int ctas_per_sm;      /* CTAs per SM of the warp-per-piece kernels; 0 = default (6) */
   uint32_t piece_width; /* neighbours per work piece: a multiple of 32, >= 32 (default 64) */
-  float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles (default 64) */
+  float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles
+                           (default 1e30: off; the autotuner tries 64) */
   float count_ms;       /* tribit_autotune: measured counting time of this setting */
 } tribit_tuning;
 tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);

@@ -117,7 +117,7 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
 void fill_schedule_stats(tribit_context* c, tribit_result* res) {
   uint32_t lens[TRIBIT_NUM_VARIANTS], hub_edges = 0;
   TB_CUDA(cudaMemcpyAsync(lens, c->sched.list_len, sizeof lens, cudaMemcpyDeviceToHost, c->st));
-  TB_CUDA(cudaMemcpyAsync(&hub_edges, c->sched.piece_off + TRIBIT_NUM_VARIANTS + 3, sizeof hub_edges,
+  TB_CUDA(cudaMemcpyAsync(&hub_edges, c->sched.piece_off + TRIBIT_NUM_VARIANTS + 4, sizeof hub_edges,
                           cudaMemcpyDeviceToHost, c->st));
   TB_CUDA(cudaStreamSynchronize(c->st));
   res->hub_edges = hub_edges;

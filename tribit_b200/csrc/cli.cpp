@@ -5,13 +5,17 @@
 // order, so the reference's benchmark harness regexes
 // (artifact/sc26/run_benchmarks/run_single_gpu.py:78-83) parse it unchanged.
 // Like the reference, a warm-up count precedes the reported one.
-// Extensions (all optional): -d <plain|learned|merge|bitmap|mma> dispatcher,
-// -o <degree|id> orientation, -m <model file> learned-dispatch weights,
-// -v extra lines after the summary block.
+// Extensions (all optional): -d <auto|plain|learned|merge|bitmap|mma>
+// dispatcher (auto, the default: learned with the weights shipped beside the
+// binary, ../models/dispatch_mlp.bin, else plain), -o <degree|id>
+// orientation, -m <model file> learned-dispatch weights, -v extra lines after
+// the summary block.
 #include <cuda_runtime.h>
 #include <getopt.h>
 #include <thrust/version.h>
 #include <cub/version.cuh>
+
+#include <unistd.h>
 
 #include <cstdio>
 #include <cstdlib>
@@ -27,7 +31,7 @@ namespace {
 struct Config {
   std::string input_file;
   std::string model;
-  int dispatch = TRIBIT_DISPATCH_PLAIN;
+  int dispatch = -1;  // auto
   int order = TRIBIT_ORDER_DEGREE;
   bool verbose = false;
 };
@@ -37,7 +41,8 @@ std::string usage(const char* prog) {
          " -i <input_file>\n"
          "Options:\n"
          "  -i <input_file>    Path to the input file (required)\n"
-         "  -d <dispatch>      plain (default), learned, merge, bitmap or mma\n"
+         "  -d <dispatch>      auto (default: learned with the bundled model, else plain),\n"
+         "                     plain, learned, merge, bitmap or mma\n"
          "  -o <order>         degree (default) or id\n"
          "  -m <model_file>    dispatcher weights for -d learned\n"
          "  -v                 print extra statistics after the summary\n";
@@ -56,7 +61,8 @@ Config options(int argc, char* argv[]) {
         cfg.input_file = optarg;
         break;
       case 'd':
-        if (!std::strcmp(optarg, "plain")) cfg.dispatch = TRIBIT_DISPATCH_PLAIN;
+        if (!std::strcmp(optarg, "auto")) cfg.dispatch = -1;
+        else if (!std::strcmp(optarg, "plain")) cfg.dispatch = TRIBIT_DISPATCH_PLAIN;
         else if (!std::strcmp(optarg, "learned")) cfg.dispatch = TRIBIT_DISPATCH_LEARNED;
         else if (!std::strcmp(optarg, "merge")) cfg.dispatch = TRIBIT_DISPATCH_MERGE;
         else if (!std::strcmp(optarg, "bitmap")) cfg.dispatch = TRIBIT_DISPATCH_BITMAP;
@@ -106,6 +112,18 @@ Config options(int argc, char* argv[]) {
   std::exit(EXIT_FAILURE);
 }
 
+// The dispatcher weights shipped with the binary: <dir of the executable>/../models/dispatch_mlp.bin.
+std::string bundled_model() {
+  char buf[4096];
+  const ssize_t k = readlink("/proc/self/exe", buf, sizeof buf - 1);
+  if (k <= 0) return {};
+  buf[k] = 0;
+  std::string dir(buf);
+  dir = dir.substr(0, dir.find_last_of('/'));
+  const std::string path = dir + "/../models/dispatch_mlp.bin";
+  return access(path.c_str(), R_OK) == 0 ? path : std::string();
+}
+
 }  // namespace
 
 int main(int argc, char* argv[]) {
@@ -120,6 +138,10 @@ int main(int argc, char* argv[]) {
   tribit_status st = tribit_read_mtx(cfg.input_file.c_str(), &n, &entries, &ne);
   if (st != TRIBIT_OK) fail(cfg.input_file.c_str(), st, nullptr);
 
+  if (cfg.dispatch < 0) {
+    if (cfg.model.empty()) cfg.model = bundled_model();
+    cfg.dispatch = cfg.model.empty() ? TRIBIT_DISPATCH_PLAIN : TRIBIT_DISPATCH_LEARNED;
+  }
   tribit_options o;
   tribit_default_options(&o);
   o.dispatch = cfg.dispatch;

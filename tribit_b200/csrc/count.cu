@@ -27,7 +27,7 @@ constexpr uint32_t kLong = 24;                       // lists at least this long
 constexpr uint32_t kGrab = 4;                        // pieces taken per cursor update
 constexpr uint64_t kEmptySlot = 0xFFFFFFFF00000000ull;
 
-enum { kCurVariant0 = 0, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6, kCurHub = 7 };
+enum { kCurVariant0 = 0, kCurHubWarp = 3, kCurCta = 4, kCurGlobal = 5, kCurHeavy = 6, kCurHub = 7 };
 // Heavy phase: CTA-shared table in the first 16 KiB of the kernel's shared
 // memory, the row's per-neighbour item prefix in the second 16 KiB.
 constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 4;
@@ -505,6 +505,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
 
 constexpr int kTileStride = kTileMaxK + 4;      // padded: fragment loads hit 32 distinct banks
 constexpr int kTileWarps = 4;
+constexpr uint32_t kTileNbrPiece = 128;         // neighbours of V per tile piece (16 groups of 8)
 struct TileSmem {
   uint32_t a[32 * kTileStride];                 // also the fallback hash table (4 KiB used)
   uint32_t b[8 * kTileStride];
@@ -548,23 +549,25 @@ __device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl
   return acc;
 }
 
-__global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, const uint8_t* __restrict__ variant_of,
-                                                               uint32_t nrb, DeviceStats* stats,
-                                                               unsigned long long* per_graph,
+__global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, const uint64_t* __restrict__ pieces,
+                                                               const uint32_t* __restrict__ piece_off,
+                                                               DeviceStats* stats, unsigned long long* per_graph,
                                                                unsigned long long* block_ns) {
   extern __shared__ __align__(16) unsigned char tile_raw[];
   TileSmem& sm = reinterpret_cast<TileSmem*>(tile_raw)[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31, grp = lane >> 2, tig = lane & 3;
+  const uint32_t p0 = piece_off[TRIBIT_VARIANT_MMA], len = piece_off[TRIBIT_VARIANT_MMA + 1] - p0;
   uint64_t acc = 0;
   for (;;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurVariant0 + TRIBIT_VARIANT_MMA], kGrab);
     t0 = __shfl_sync(kFull, t0, 0);
-    if (t0 >= nrb) break;
-    const uint32_t t1 = min(t0 + kGrab, nrb);
+    if (t0 >= len) break;
+    const uint32_t t1 = min(t0 + kGrab, len);
     for (uint32_t t = t0; t < t1; ++t) {
-      const uint32_t rb = nrb - 1 - t;
-      if (variant_of[rb] != TRIBIT_VARIANT_MMA) continue;
+      // A piece is (first row of the block << 32) | index of its first neighbour in V.
+      const uint64_t pc = pieces[p0 + (len - 1 - t)];
+      const uint32_t rb = (uint32_t)(pc >> 32) >> 5, first = (uint32_t)pc;
       const unsigned long long t_start = (block_ns && lane == 0) ? cycles() : 0ull;
       // Row of this lane: activity and block range.
       const uint32_t u = rb * 32 + lane;
@@ -590,7 +593,8 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
       const uint32_t K = hi - lo + 1;
       uint64_t racc = 0;
       if (K > (uint32_t)kTileMaxK) {
-        racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), per_graph);
+        // Forced onto a block that fits no tile: its one piece sweeps the rows.
+        if (first == 0) racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), per_graph);
       } else {
         const uint32_t KP = (K + 7) & ~7u;  // words, whole 256-bit k-steps
         for (uint32_t i = lane; i < 32 * kTileStride; i += 32) sm.a[i] = 0u;
@@ -615,7 +619,18 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
         __syncwarp();
         int rowsum[4] = {0, 0, 0, 0};  // rows grp, grp + 8, 16 + grp, 24 + grp
         uint32_t cw = 0, cbits = sm.vmask[0];  // warp-uniform cursor over V's set bits
-        for (;;) {
+        // This piece's neighbours: V[first, first + kTileNbrPiece).
+        for (uint32_t skip = first; skip > 0;) {
+          const uint32_t c = __popc(cbits);
+          if (c > skip) {
+            for (uint32_t q = 0; q < skip; ++q) cbits &= cbits - 1;
+            break;
+          }
+          skip -= c;
+          cbits = cw + 1 < K ? sm.vmask[++cw] : 0u;
+          if (cbits == 0 && cw + 1 >= K) break;
+        }
+        for (uint32_t done = 0; done < kTileNbrPiece; done += 8) {
           // Next 8 neighbours, as column offsets from lo * 32 (0xFFFF = none).
           uint32_t vc[8];
           uint32_t nv = 0;
@@ -802,8 +817,10 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 // hub) and flags it so the row sweeps skip it. A CTA then stages v's bit row
 // once as a direct-mapped array of masks over its block span, and its warps
 // walk the tails of a piece of v's in-edges against it: per tail block one
-// shared-memory load, AND and popc, and no search. Every edge is counted
-// exactly once, here or by its row.
+// shared-memory load, AND and popc, and no search. Hubs whose span fits a
+// warp's slice of the map (kHubWarpSpan blocks) are staged and walked by one
+// warp alone, with no CTA barrier per piece. Every edge is counted exactly
+// once, here or by its row.
 
 // Build-time tunables (-D...): measured defaults.
 #ifndef TB_HUB_PIECE
@@ -814,7 +831,9 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 #endif
 constexpr int kHubWarps = 8;
 constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
-constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per piece
+constexpr uint32_t kHubWarpSpan = kHubMaxSpan / kHubWarps;  // spans up to this: one warp per piece
+constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per CTA piece
+constexpr uint32_t kHubWarpPiece = 256;         // in-edges per warp piece
 constexpr int kHubCtasPerSm = 5;
 constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lane
 
@@ -830,8 +849,10 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
   __shared__ uint32_t s_t;
   __shared__ unsigned long long s_dt;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const uint32_t len = piece_off[TRIBIT_NUM_VARIANTS + 2];
+  const uint32_t len = piece_off[TRIBIT_NUM_VARIANTS + 2];  // CTA pieces; warp pieces follow them
+  const uint32_t wlen = piece_off[TRIBIT_NUM_VARIANTS + 3] - len;
   uint64_t acc = 0;
+  // Phase 1: hubs with wide rows, one CTA per piece.
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(&stats->cursor[kCurHub], 1u);
     __syncthreads();
@@ -911,6 +932,58 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
         atomicAdd(&block_ns[inrow[e0 + i] >> 5], (unsigned long long)(per_block * (pre[i + 1] - pre[i]) + 0.5));
       __syncthreads();
     }
+  }
+  // Phase 2: hubs whose span fits a warp's slice of the map, one warp per
+  // piece, largest hubs first.
+  uint32_t* wmap = map + w * kHubWarpSpan;
+  for (;;) {
+    uint32_t t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurHubWarp], 1u);
+    const uint32_t t = __shfl_sync(kFull, t0, 0);
+    if (t >= wlen) break;
+    const unsigned long long t_start = block_ns ? cycles() : 0ull;
+    const uint64_t pc = hub_pieces[len + wlen - 1 - t];
+    const uint32_t v = (uint32_t)(pc >> 32);
+    const uint32_t e0 = in_off[v] + (uint32_t)pc;
+    const uint32_t cnt = min(kHubWarpPiece, in_off[v + 1] - e0);
+    const uint64_t a = g.rp[v], b = g.rp[v + 1];
+    const uint32_t bs = rp_blk(a), be = rp_blk(b);
+    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32);
+    const uint32_t span = (uint32_t)(g.bent[be - 1] >> 32) - bmin + 1;  // <= kHubWarpSpan by the schedule
+    for (uint32_t i = lane; i < span; i += 32) wmap[i] = 0u;
+    __syncwarp();
+    for (uint32_t k = bs + lane; k < be; k += 32) {
+      const uint64_t e = g.bent[k];
+      wmap[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+    }
+    __syncwarp();
+    const uint64_t racc = sweep_flat<kHubDepth>(
+        0, cnt, 0, 1,
+        [&](uint32_t i, uint32_t& ib, uint32_t& il) {
+          const uint64_t x = inl[e0 + i];
+          ib = (uint32_t)(x >> 32);
+          il = (uint32_t)x;
+        },
+        [&](uint32_t k) -> uint64_t { return g.bent[k]; },
+        [&](uint64_t e) -> uint32_t {
+          const uint32_t o = (uint32_t)(e >> 32) - bmin;
+          return o < span ? (uint32_t)__popc((uint32_t)e & wmap[o]) : 0u;
+        });
+    if (per_graph) {
+      const uint64_t s = warp_sum(racc);
+      if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
+    }
+    acc += racc;
+    if (block_ns) {
+      // The piece's cycles, shared among its in-edges' row blocks by tail length.
+      uint32_t tot = 0;
+      for (uint32_t i = lane; i < cnt; i += 32) tot += (uint32_t)inl[e0 + i];
+      tot = warp_sum(tot);
+      const double per_block = (double)(cycles() - t_start) / (double)max(tot, 1u);
+      for (uint32_t i = lane; i < cnt; i += 32)
+        atomicAdd(&block_ns[inrow[e0 + i] >> 5], (unsigned long long)(per_block * (uint32_t)inl[e0 + i] + 0.5));
+    }
+    __syncwarp();  // the slice is rewritten for the next piece
   }
   acc = warp_sum(acc);
   if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
@@ -1036,13 +1109,62 @@ __global__ void k_heavy_scatter(GraphView g, const uint32_t* __restrict__ pos, u
   if (u == g.n) piece_off[TRIBIT_NUM_VARIANTS + 1] = pos[g.n];
 }
 
-// Pieces of each row block (one warp per row block).
-__global__ void k_block_pieces(GraphView g, uint32_t nrb, uint32_t* __restrict__ cnt, uint32_t width) {
+// Pieces of a bit-tile row block: its neighbour set V (the OR of the active
+// rows' bit rows over the block's column range) in chunks of kTileNbrPiece;
+// one piece when the rows span more than kTileMaxK blocks (swept row by
+// row). vm: kTileMaxK words of this warp's shared memory.
+__device__ uint32_t tile_pieces(const GraphView& g, uint32_t rb, uint32_t* vm) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t u = rb * 32 + lane;
+  uint32_t bs = 0, be = 0, lo = 0xFFFFFFFFu, hi = 0;
+  bool active = false;
+  if (u < g.n) {
+    const uint64_t a = g.rp[u], b = g.rp[u + 1];
+    bs = rp_blk(a);
+    be = rp_blk(b);
+    active = rp_row(b) - rp_row(a) >= 2 && be - bs <= kWarpMaxBlocks;
+    if (active) {
+      lo = (uint32_t)(g.bent[bs] >> 32);
+      hi = (uint32_t)(g.bent[be - 1] >> 32);
+    }
+  }
+  const uint32_t amask = __ballot_sync(kFull, active);
+  if (!amask) return 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+    hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+  }
+  if (hi - lo + 1 > (uint32_t)kTileMaxK) return 1u;
+  for (uint32_t i = lane; i < (uint32_t)kTileMaxK; i += 32) vm[i] = 0u;
+  __syncwarp();
+  for (uint32_t r = 0; r < 32; ++r) {
+    if (!((amask >> r) & 1u)) continue;
+    const uint32_t rbs = __shfl_sync(kFull, bs, r), rbe = __shfl_sync(kFull, be, r);
+    for (uint32_t k = rbs + lane; k < rbe; k += 32) {
+      const uint64_t e = g.bent[k];
+      atomicOr(&vm[(uint32_t)(e >> 32) - lo], (uint32_t)e);
+    }
+  }
+  __syncwarp();
+  uint32_t c = 0;
+  for (uint32_t i = lane; i < (uint32_t)kTileMaxK; i += 32) c += __popc(vm[i]);
+  c = warp_sum(c);
+  __syncwarp();
+  return (c + kTileNbrPiece - 1) / kTileNbrPiece;
+}
+
+// Pieces of each row block (one warp per row block): bit-tile blocks by
+// tile_pieces, the others one per piece_width neighbours of each row.
+__global__ void __launch_bounds__(256) k_block_pieces(GraphView g, uint32_t nrb, const uint8_t* __restrict__ variant_of,
+                                                      uint32_t* __restrict__ cnt, uint32_t width) {
+  __shared__ uint32_t vm[8][kTileMaxK];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
-    const uint32_t s = warp_sum(row_pieces(g, rb * 32 + lane, width));
+    const uint32_t s = variant_of[rb] == TRIBIT_VARIANT_MMA ? tile_pieces(g, rb, vm[threadIdx.x >> 5])
+                                                            : warp_sum(row_pieces(g, rb * 32 + lane, width));
     if (lane == 0) cnt[rb] = s;
   }
 }
@@ -1070,6 +1192,11 @@ __global__ void k_piece_scatter(GraphView g, uint32_t nrb, const uint8_t* __rest
   const uint32_t seg = piece_off[v];
   for (uint32_t rb = warp; rb < nrb; rb += nwarps) {
     if (variant_of[rb] != v) continue;
+    if (v == TRIBIT_VARIANT_MMA) {
+      const uint32_t base = seg + off[rb], np = off[rb + 1] - off[rb];
+      for (uint32_t k = lane; k < np; k += 32) pieces[base + k] = ((uint64_t)(rb * 32) << 32) | (k * kTileNbrPiece);
+      continue;
+    }
     const uint32_t u = rb * 32 + lane;
     const uint32_t np = row_pieces(g, u, width);
     const uint32_t incl = warp_inclusive_sum(np);
@@ -1157,24 +1284,44 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   }
 }
 
-// Pieces per hub: ceil(in-edges / kHubPiece); cnt[n] = 0 for the scan.
-__global__ void k_hub_piece_count(const uint32_t* __restrict__ in_off, uint32_t n, uint32_t* __restrict__ cnt) {
+// Pieces per hub, 2n + 2 counts: cnt[v] CTA pieces of ceil(in-edges /
+// kHubPiece) for hubs wider than a warp's slice, cnt[n + 1 + v] warp pieces
+// of ceil(in-edges / kHubWarpPiece) for the rest; cnt[n] = cnt[2n + 1] = 0.
+// One exclusive scan places every CTA piece before every warp piece.
+__global__ void k_hub_piece_count(const uint32_t* __restrict__ in_off, const uint64_t* __restrict__ vinfo,
+                                  uint32_t n, uint32_t* __restrict__ cnt) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v > n) return;
-  cnt[v] = v < n ? (in_off[v + 1] - in_off[v] + kHubPiece - 1) / kHubPiece : 0u;
+  uint32_t c = 0, wc = 0;
+  if (v < n) {
+    const uint32_t k = in_off[v + 1] - in_off[v];
+    if ((uint32_t)(vinfo[v] >> 32) <= kHubWarpSpan)
+      wc = (k + kHubWarpPiece - 1) / kHubWarpPiece;
+    else
+      c = (k + kHubPiece - 1) / kHubPiece;
+  }
+  cnt[v] = c;
+  cnt[n + 1 + v] = wc;
 }
 
 __global__ void k_hub_piece_scatter(const uint32_t* __restrict__ pos, uint32_t n, uint64_t* __restrict__ pieces,
                                     uint32_t* __restrict__ piece_off) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < n)
+  if (v < n) {
     for (uint32_t k = 0, np = pos[v + 1] - pos[v]; k < np; ++k)
       pieces[pos[v] + k] = ((uint64_t)v << 32) | (k * kHubPiece);
-  if (v == n) piece_off[TRIBIT_NUM_VARIANTS + 2] = pos[n];
+    const uint32_t* wpos = pos + n + 1;
+    for (uint32_t k = 0, np = wpos[v + 1] - wpos[v]; k < np; ++k)
+      pieces[wpos[v] + k] = ((uint64_t)v << 32) | (k * kHubWarpPiece);
+  }
+  if (v == n) {
+    piece_off[TRIBIT_NUM_VARIANTS + 2] = pos[n];          // CTA pieces
+    piece_off[TRIBIT_NUM_VARIANTS + 3] = pos[2 * n + 1];  // all pieces
+  }
 }
 
 __global__ void k_hub_total(const uint32_t* __restrict__ in_off, uint32_t n, uint32_t* __restrict__ piece_off) {
-  piece_off[TRIBIT_NUM_VARIANTS + 3] = in_off[n];
+  piece_off[TRIBIT_NUM_VARIANTS + 4] = in_off[n];
 }
 
 }  // namespace
@@ -1184,9 +1331,9 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
   const uint32_t nrb = (uint32_t)ceil_div<uint64_t>(n, 32);
   s.num_row_blocks = nrb;
   s.variant_of = ar.take<uint8_t>(nrb + 1);
-  s.piece_cap = n + E / kMinPieceWidth + 64;
+  s.piece_cap = 2 * n + E / kMinPieceWidth + 64;  // row pieces, plus up to 16 per bit-tile block
   s.pieces = ar.take<uint64_t>(s.piece_cap);
-  s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 4);
+  s.piece_off = ar.take<uint32_t>(TRIBIT_NUM_VARIANTS + 5);
   s.heavy = ar.take<uint32_t>(n + 1);
   s.row_flags = ar.take<uint32_t>(n + 1);
   s.row_scan_tmp = take_scan_temp<uint32_t>(ar, n + 1);
@@ -1206,17 +1353,19 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.in_off = ar.take<uint32_t>(n + 1);
     s.inl = ar.take<uint64_t>(E + 1);
     s.inrow = ar.take<uint32_t>(E + 1);
-    s.hub_pieces = ar.take<uint64_t>(n + E / kHubPiece + 64);
+    s.hub_pieces = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
+    s.hub_pos = ar.take<uint32_t>(2 * (n + 1));
+    s.hub_scan_tmp = take_scan_temp<uint32_t>(ar, 2 * (n + 1));
   }
   return s;
 }
 
 // Hub in-lists and pieces of the merge row blocks (after the heavy-row list:
-// row_flags and its scan space are reused). Without hub arrays, or with
-// hubs off, the hub pass gets no pieces and no edge is flagged.
+// its scan space is reused for the in-list offsets). Without hub arrays, or
+// with hubs off, the hub pass gets no pieces and no edge is flagged.
 static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   s.hubs_active = false;
-  TB_CUDA(cudaMemsetAsync(s.piece_off + TRIBIT_NUM_VARIANTS + 2, 0, 2 * sizeof(uint32_t), st));
+  TB_CUDA(cudaMemsetAsync(s.piece_off + TRIBIT_NUM_VARIANTS + 2, 0, 3 * sizeof(uint32_t), st));
   if (!s.eflag || !s.hubs || g.n == 0) return;
   const uint64_t n = g.n;
   const unsigned vblocks = (unsigned)ceil_div<uint64_t>(n + 1, 256);
@@ -1237,10 +1386,10 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
                                            s.inrow);
   TB_LAUNCH_CHECK();
-  k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, (uint32_t)n, s.row_flags);
+  k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, s.vinfo, (uint32_t)n, s.hub_pos);
   TB_LAUNCH_CHECK();
-  device_scan<uint32_t, OpSum>(s.row_flags, s.row_flags, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
-  k_hub_piece_scatter<<<vblocks, 256, 0, st>>>(s.row_flags, (uint32_t)n, s.hub_pieces, s.piece_off);
+  device_scan<uint32_t, OpSum>(s.hub_pos, s.hub_pos, 2 * (n + 1), true, OpSum{}, 0u, s.hub_scan_tmp, st);
+  k_hub_piece_scatter<<<vblocks, 256, 0, st>>>(s.hub_pos, (uint32_t)n, s.hub_pieces, s.piece_off);
   TB_LAUNCH_CHECK();
   k_hub_total<<<1, 1, 0, st>>>(s.in_off, (uint32_t)n, s.piece_off);
   TB_LAUNCH_CHECK();
@@ -1253,7 +1402,7 @@ void build_pieces(const GraphView& g, Schedule& s, cudaStream_t st) {
   const unsigned fblocks = (unsigned)ceil_div<uint64_t>(nrb + 1, 256);
   TB_CUDA(cudaMemsetAsync(s.list_len, 0, TRIBIT_NUM_VARIANTS * sizeof(uint32_t), st));
   if (nrb) {
-    k_block_pieces<<<wblocks, 256, 0, st>>>(g, nrb, s.block_pieces, s.piece_width);
+    k_block_pieces<<<wblocks, 256, 0, st>>>(g, nrb, s.variant_of, s.block_pieces, s.piece_width);
     TB_LAUNCH_CHECK();
   }
   for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) {
@@ -1318,7 +1467,7 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
       g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy, s.piece_width);
   TB_LAUNCH_CHECK();
   k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
-      g, s.variant_of, s.num_row_blocks, stats, per_graph, cfg.block_ns);
+      g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
                                                                                per_graph, cfg.block_ns, nullptr,

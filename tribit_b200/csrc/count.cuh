@@ -32,7 +32,7 @@ struct Schedule {
   uint64_t* pieces = nullptr;      // device, (row << 32) | first neighbour, grouped by variant
   uint64_t piece_cap = 0;
   uint32_t* piece_off = nullptr;   // device, TRIBIT_NUM_VARIANTS + 1 segment starts, the heavy-row count,
-                                   // the hub-piece count, the hub-edge count
+                                   // the CTA hub-piece count, all hub pieces, the hub-edge count
   uint32_t* heavy = nullptr;       // device, rows too wide for one warp, counted CTA-cooperatively first
   uint32_t* row_flags = nullptr;   // device, n + 1 scratch for the heavy-row scan
   uint32_t* row_scan_tmp = nullptr;
@@ -52,11 +52,13 @@ struct Schedule {
   uint32_t* in_off = nullptr;      // device, n + 1: in-list of hub v at [in_off[v], in_off[v+1])
   uint64_t* inl = nullptr;         // device: (first block of u's tail << 32) | tail length
   uint32_t* inrow = nullptr;       // device: u of each in-list entry
-  uint64_t* hub_pieces = nullptr;  // device: (v << 32) | first in-list entry
+  uint64_t* hub_pieces = nullptr;  // device: (v << 32) | first in-list entry; CTA pieces, then warp pieces
+  uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
+  uint32_t* hub_scan_tmp = nullptr;
   bool hubs = true;                // build the hub lists for merge row blocks
   bool hubs_active = false;        // set by build_pieces
   uint32_t piece_width = 64;       // neighbours per piece (tuned)
-  float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
+  float tile_min_nnz = 1e30f;      // plain dispatcher: fewest edges for a bit-tile row block (tuned)
   const void* model = nullptr;     // device MLP parameters for learned dispatch
 };
 

@@ -30,42 +30,32 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "models", "dispatch_mlp.bin")
 
 
-def batch_union(num_graphs: int, seed: int):
-    """Disjoint union of small ER / Chung-Lu graphs (the batched workload's mix)."""
-    rng = np.random.default_rng(seed)
-    parts, base = [], 0
-    for g in range(num_graphs):
-        n = int(round(64 * 1024 ** rng.uniform()))
-        d = rng.uniform(8, 64)
-        if rng.uniform() < 0.5:
-            e = tb.gen_er(n, int(n * d / 2), seed=seed * 100003 + g)
-        else:
-            e = tb.gen_chung_lu(n, int(n * d / 2), float(rng.uniform(2.1, 2.8)), max(4.0, n / 8), seed=seed * 100003 + g)
-        hi = (e >> np.uint64(32)) + np.uint64(base)
-        lo = (e & np.uint64(0xFFFFFFFF)) + np.uint64(base)
-        parts.append((hi << np.uint64(32)) | lo)
-        base += n
-    return base, np.concatenate(parts)
-
-
 def training_graphs(quick: bool):
+    """(name, make) pairs; make() returns ("graph", n, entries) or ("batch",
+    entries, offsets, num_nodes) -- batches are prepared as the batched
+    workload is, graph by graph (tribit_count_batch)."""
+    def rmat(scale, seed):
+        return lambda: ("graph", 1 << scale, tb.gen_rmat(scale, 16, seed=seed))
+
+    def planted(c, seed):
+        return lambda: ("graph", c * 100, tb.gen_planted(c, 100, 0.3, 2, seed=seed))
+
+    def batch(g, seed):
+        return lambda: ("batch", *tb.gen_batch(g, seed=seed))
+
     if quick:
-        return [("rmat18_s118", lambda: (1 << 18, tb.gen_rmat(18, 16, seed=118))),
-                ("planted_s103", lambda: (400_000, tb.gen_planted(4000, 100, 0.3, 2, seed=103))),
-                ("batch_s101", lambda: batch_union(64, 101))]
-    return [("rmat22_s122", lambda: (1 << 22, tb.gen_rmat(22, 16, seed=122))),
-            ("rmat21_s121", lambda: (1 << 21, tb.gen_rmat(21, 16, seed=121))),
-            ("planted_s103", lambda: (2_000_000, tb.gen_planted(20000, 100, 0.3, 2, seed=103))),
-            ("batch_s101", lambda: batch_union(512, 101))]
+        return [("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(4000, 103)), ("batch_s101", batch(64, 101))]
+    return [("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)), ("planted_s103", planted(20000, 103)),
+            ("batch_s101", batch(1024, 101))]
 
 
 def holdout_graph(quick: bool):
     if quick:
-        return "rmat17_s7", (1 << 17, tb.gen_rmat(17, 16, seed=7))
-    return "rmat22_s7", (1 << 22, tb.gen_rmat(22, 16, seed=7))
+        return "rmat17_s7", ("graph", 1 << 17, tb.gen_rmat(17, 16, seed=7))
+    return "rmat22_s7", ("graph", 1 << 22, tb.gen_rmat(22, 16, seed=7))
 
 
-def collect(n, e, repeats: int = 2):
+def collect(item, repeats: int = 2):
     """Features and per-row-block cost (ns) of each variant.
 
     A row block's SM cycles measure how long its warp worked, not what it cost
@@ -74,9 +64,13 @@ def collect(n, e, repeats: int = 2):
     variant's cycles are scaled to its measured device time: cost of block b
     = cycles_b / sum of cycles * time of the variant kernels."""
     import torch
-    d = torch.from_numpy(e.view(np.int64)).cuda()
     with tb.Counter(dispatch="plain") as c:
-        c.prepare_device(d.data_ptr(), d.numel(), n)
+        if item[0] == "batch":
+            c.count_batch(*item[1:])
+        else:
+            _, n, e = item
+            d = torch.from_numpy(e.view(np.int64)).cuda()
+            c.prepare_device(d.data_ptr(), d.numel(), n)
         x = c.block_features()
         costs, tri = [], set()
         for v in tb.VARIANTS:
@@ -147,8 +141,7 @@ def main():
     xs, ys = [], []
     for name, make in training_graphs(args.quick):
         t0 = time.time()
-        n, e = make()
-        x, t, _, _ = collect(n, e)
+        x, t, _, _ = collect(make())
         xs.append(x)
         ys.append(np.log2(1.0 + t))
         print(json.dumps({"graph": name, "row_blocks": int(x.shape[0]), "seconds": round(time.time() - t0, 1),
@@ -157,8 +150,9 @@ def main():
     Y = np.concatenate(ys).astype(np.float32)
     norm = np.concatenate([X.mean(0), X.std(0) + 1e-3, Y.mean(0), Y.std(0) + 1e-3]).astype(np.float32)
 
-    hname, (hn, he) = holdout_graph(args.quick)
-    hx, ht, _, _ = collect(hn, he)
+    hname, hitem = holdout_graph(args.quick)
+    _, hn, he = hitem
+    hx, ht, _, _ = collect(hitem)
     with tb.Counter() as c:
         c.model_init(norm, seed=args.seed)
         loss = c.model_train(X, Y, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed)
