@@ -188,6 +188,54 @@ __device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, uint32_
   return acc;
 }
 
+// The same flattening with the owner found incrementally: the chunk's
+// inclusive prefix and item offsets go to the warp's 64 words of shared
+// memory (wsm), each lane finds the owner of its first item once by binary
+// search and then only advances it (items of a lane only grow), so a long
+// list costs one shared-memory compare per item instead of a 5-step search.
+template <int Depth, class Desc, class Load, class Probe>
+__device__ __forceinline__ uint64_t sweep_runs(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
+                                               const Desc& desc, const Load& load, const Probe& probe,
+                                               uint32_t* wsm) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t acc = 0;
+  for (uint32_t c = cs + chunk0 * 32; c < ce; c += step * 32) {
+    const uint32_t j = c + lane;
+    uint32_t ib = 0, il = 0;
+    if (j < ce) desc(j, ib, il);
+    const uint32_t incl = warp_inclusive_sum(il);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    __syncwarp();
+    wsm[lane] = incl;
+    wsm[32 + lane] = ib - (incl - il);  // item t of the chunk, owned by slot s, is item off_s + t
+    __syncwarp();
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t st = 16; st >= 1; st >>= 1)
+      if (wsm[s + st - 1] <= lane) s += st;
+    uint32_t lim = wsm[s], off = wsm[32 + s];
+    uint32_t racc = 0;
+    for (uint32_t base = 0; base < total; base += 32 * Depth) {
+      uint64_t x[Depth];
+#pragma unroll
+      for (int r = 0; r < Depth; ++r) {
+        const uint32_t t = base + 32 * r + lane;
+        while (t >= lim && s < 31) {
+          ++s;
+          lim = wsm[s];
+          off = wsm[32 + s];
+        }
+        x[r] = t < total ? load(off + t) : 0ull;
+      }
+#pragma unroll
+      for (int r = 0; r < Depth; ++r) racc += probe(x[r]);
+    }
+    acc += racc;
+  }
+  __syncwarp();
+  return acc;
+}
+
 // Edge j of the CSR is counted by the hub pass (see k_hub) instead of by its
 // row's sweep.
 __device__ __forceinline__ bool edge_to_hub(const GraphView& g, uint32_t j) {
@@ -212,8 +260,8 @@ __device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint3
 }
 
 // Bit-row sweep: every bit block of v = col[j], j in the slots, scored by
-// probe (a hash or direct-map lookup in u's staged row). Flattened with
-// kBitsDepth blocks in flight per lane (see sweep_flat).
+// probe (a hash or direct-map lookup in u's staged row), flattened with
+// kBitsDepth blocks in flight per lane (sweep_runs; wsm: the warp's 64 words).
 #ifndef TB_BITS_DEPTH
 #define TB_BITS_DEPTH 4
 #endif
@@ -221,10 +269,8 @@ constexpr int kBitsDepth = TB_BITS_DEPTH;
 
 template <class Probe>
 __device__ __forceinline__ uint64_t sweep_bits(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
-                                               uint32_t step, const Probe& probe) {
-  if (kBitsDepth == 0)
-    return sweep<true>(g, cs, ce, chunk0, step, [&](uint32_t k, uint32_t) -> uint32_t { return probe(g.bent[k]); });
-  return sweep_flat<kBitsDepth == 0 ? 1 : kBitsDepth>(
+                                               uint32_t step, const Probe& probe, uint32_t* wsm) {
+  return sweep_runs<kBitsDepth>(
       cs, ce, chunk0, step,
       [&](uint32_t j, uint32_t& ib, uint32_t& il) {
         if (edge_to_hub(g, j)) return;
@@ -233,7 +279,7 @@ __device__ __forceinline__ uint64_t sweep_bits(const GraphView& g, uint32_t cs, 
         ib = rp_blk(a);
         il = rp_blk(b) - ib;
       },
-      [&](uint32_t k) -> uint64_t { return g.bent[k]; }, probe);
+      [&](uint32_t k) -> uint64_t { return g.bent[k]; }, probe, wsm);
 }
 
 // Mask of block x in the sorted bit row r[lo, end), or 0.
@@ -342,6 +388,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
                                                                     const uint32_t* __restrict__ heavy,
                                                                     uint32_t width) {
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
+  __shared__ uint32_t runs[kWarpsPerCta][64];
   __shared__ uint32_t s_row;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* tbl = smem[w];
@@ -412,7 +459,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kWarpsPerCta));
       const uint32_t ce = w + 1 == kWarpsPerCta ? d : first_at((uint32_t)((uint64_t)tot * (w + 1) / kWarpsPerCta));
       const BitmapProbe probe{ctbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
-      const uint64_t racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe);
+      const uint64_t racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe, runs[w]);
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
         if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
@@ -475,7 +522,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         racc = sweep_merge(g, tbl, d, cs, ce);
       } else {
         const BitmapProbe probe{tbl, logb, bmin, bmax};
-        racc = sweep_bits(g, cs, ce, 0, 1, probe);
+        racc = sweep_bits(g, cs, ce, 0, 1, probe, runs[w]);
       }
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
@@ -522,7 +569,8 @@ __device__ __forceinline__ void mma_b1(int (&c)[4], uint32_t a0, uint32_t a1, ui
 }
 
 // Per-row bitmap sweep of the active rows of a row block (the fallback).
-__device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl, unsigned long long* per_graph) {
+__device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl, uint32_t* wsm,
+                                  unsigned long long* per_graph) {
   const uint32_t lane = threadIdx.x & 31;
   uint64_t acc = 0;
   for (uint32_t r = 0; r < 32; ++r) {
@@ -539,7 +587,7 @@ __device__ uint64_t tile_fallback(const GraphView& g, uint32_t rb, uint64_t* tbl
     __syncwarp();
     const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
     const uint64_t racc =
-        sweep_bits(g, rs, re, 0, 1, probe);
+        sweep_bits(g, rs, re, 0, 1, probe, wsm);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
@@ -594,7 +642,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
       uint64_t racc = 0;
       if (K > (uint32_t)kTileMaxK) {
         // Forced onto a block that fits no tile: its one piece sweeps the rows.
-        if (first == 0) racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), per_graph);
+        if (first == 0) racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), sm.b, per_graph);
       } else {
         const uint32_t KP = (K + 7) & ~7u;  // words, whole 256-bit k-steps
         for (uint32_t i = lane; i < 32 * kTileStride; i += 32) sm.a[i] = 0u;
@@ -734,6 +782,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_cta(GraphView g, const uin
                                                            unsigned long long* per_graph,
                                                            unsigned long long* block_ns) {
   extern __shared__ __align__(16) uint64_t tbl[];
+  __shared__ uint32_t runs[kCtaThreads / 32][64];
   __shared__ uint32_t s_t;
   const uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t len = stats->overflow[kOvfCta];
@@ -759,7 +808,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_cta(GraphView g, const uin
     __syncthreads();
     const BitmapProbe probe{tbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
     const uint64_t racc =
-        sweep_bits(g, rs, re, w, nw, probe);
+        sweep_bits(g, rs, re, w, nw, probe, runs[w]);
     const uint64_t s = block_sum_u64(racc);  // also the barrier before the table is rebuilt
     if (threadIdx.x == 0) {
       if (per_graph && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
@@ -817,7 +866,9 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 // hub) and flags it so the row sweeps skip it. A CTA then stages v's bit row
 // once as a direct-mapped array of masks over its block span, and its warps
 // walk the tails of a piece of v's in-edges against it: per tail block one
-// shared-memory load, AND and popc, and no search. Hubs whose span fits a
+// shared-memory load, AND and popc, and no search. A hub row spanning more
+// than kHubMaxSpan blocks but holding at most kHubMaxHash blocks is staged as
+// a bucketed hash instead (one bucket load per tail block). Hubs whose row fits a
 // warp's slice of the map (kHubWarpSpan blocks) are staged and walked by one
 // warp alone, with no CTA barrier per piece. Every edge is counted exactly
 // once, here or by its row.
@@ -832,10 +883,49 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 constexpr int kHubWarps = 8;
 constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
 constexpr uint32_t kHubWarpSpan = kHubMaxSpan / kHubWarps;  // spans up to this: one warp per piece
+// Rows spanning more than that are staged as a bucketed hash instead (the same
+// 32 KiB, or a warp's 4 KiB slice, as 8-byte slots at most half full).
+constexpr uint32_t kHubMaxHash = kHubMaxSpan / 4;          // bit blocks: CTA hash
+#ifndef TB_HUB_HASH_MUL
+#define TB_HUB_HASH_MUL 4
+#endif
+#ifndef TB_HUB_HASH_MIN
+#define TB_HUB_HASH_MIN 1024
+#endif
+constexpr uint32_t kHubHashMul = TB_HUB_HASH_MUL;  // hashed hubs must save this many times their staging
+constexpr uint32_t kHubHashMin = TB_HUB_HASH_MIN;  // ... plus this many blocks (0 / 0: no hashed hubs)
+constexpr uint32_t kHubWarpHash = kHubWarpSpan / 4;        // bit blocks: warp hash
 constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per CTA piece
 constexpr uint32_t kHubWarpPiece = 256;         // in-edges per warp piece
+#ifndef TB_HUB_WAVES
+#define TB_HUB_WAVES 32
+#endif
+constexpr uint32_t kHubWaves = TB_HUB_WAVES;    // row ranges the hub pieces are ordered by (power of 2)
 constexpr int kHubCtasPerSm = 5;
 constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lane
+
+// Walks the tails of in-list entries [cs, ce) (at list) against v's staged row:
+// direct-mapped masks over blocks [bmin, bmin + span) in map, or a bucketed
+// hash (map as 8-byte slots, 2^logb buckets).
+__device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t* __restrict__ list, uint32_t cs,
+                                              uint32_t ce, bool direct, const uint32_t* map, uint32_t bmin,
+                                              uint32_t bmax, int logb, uint32_t* wsm) {
+  auto desc = [&](uint32_t i, uint32_t& ib, uint32_t& il) {
+    const uint64_t x = list[i];
+    ib = (uint32_t)(x >> 32);
+    il = (uint32_t)x;
+  };
+  auto load = [&](uint32_t k) -> uint64_t { return g.bent[k]; };
+  if (direct) {
+    const uint32_t span = bmax - bmin + 1;
+    return sweep_runs<kHubDepth>(cs, ce, 0, 1, desc, load, [&](uint64_t e) -> uint32_t {
+      const uint32_t o = (uint32_t)(e >> 32) - bmin;
+      return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
+    }, wsm);
+  }
+  const BitmapProbe probe{reinterpret_cast<const uint64_t*>(map), logb, bmin, bmax};
+  return sweep_runs<kHubDepth>(cs, ce, 0, 1, desc, load, probe, wsm);
+}
 
 __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
@@ -844,8 +934,9 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
                                                         const uint32_t* __restrict__ inrow, DeviceStats* stats,
                                                         unsigned long long* per_graph,
                                                         unsigned long long* block_ns) {
-  __shared__ uint32_t map[kHubMaxSpan];
+  __shared__ __align__(16) uint32_t map[kHubMaxSpan];
   __shared__ uint32_t pre[kHubPiece + 1];
+  __shared__ uint32_t runs[kHubWarps][64];
   __shared__ uint32_t s_t;
   __shared__ unsigned long long s_dt;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -859,21 +950,32 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     const uint32_t t = s_t;
     if (t >= len) break;
     const unsigned long long t_start = block_ns ? cycles() : 0ull;
-    // Largest hubs first: pieces are in ascending v.
-    const uint64_t pc = hub_pieces[len - 1 - t];
+    // Pieces are in wave order (see k_wave_bounds).
+    const uint64_t pc = hub_pieces[t];
     const uint32_t v = (uint32_t)(pc >> 32);
     const uint32_t e0 = in_off[v] + (uint32_t)pc;
     const uint32_t cnt = min(kHubPiece, in_off[v + 1] - e0);
     const uint64_t a = g.rp[v], b = g.rp[v + 1];
     const uint32_t bs = rp_blk(a), be = rp_blk(b);
-    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32);
-    const uint32_t span = (uint32_t)(g.bent[be - 1] >> 32) - bmin + 1;  // <= kHubMaxSpan by the schedule
-    for (uint32_t i = threadIdx.x; i < span; i += blockDim.x) map[i] = 0u;
+    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32), bmax = (uint32_t)(g.bent[be - 1] >> 32);
+    const uint32_t span = bmax - bmin + 1;
+    const bool direct = span <= kHubMaxSpan;  // else be - bs <= kHubMaxHash (schedule)
+    uint64_t* htbl = reinterpret_cast<uint64_t*>(map);
+    const int logb = table_logb(be - bs);
+    if (direct) {
+      for (uint32_t i = threadIdx.x; i < span; i += blockDim.x) map[i] = 0u;
+    } else {
+      table_clear(htbl, logb, threadIdx.x, blockDim.x);
+    }
     for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) pre[i] = (uint32_t)inl[e0 + i];
     __syncthreads();
-    for (uint32_t k = bs + threadIdx.x; k < be; k += blockDim.x) {
-      const uint64_t e = g.bent[k];
-      map[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+    if (direct) {
+      for (uint32_t k = bs + threadIdx.x; k < be; k += blockDim.x) {
+        const uint64_t e = g.bent[k];
+        map[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+      }
+    } else {
+      table_insert(htbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
     }
     // Tail-length prefix: pre[i] = blocks of the tails before i, pre[cnt] = all.
     {
@@ -905,18 +1007,7 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     };
     const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kHubWarps));
     const uint32_t ce = w + 1 == kHubWarps ? cnt : first_at((uint32_t)((uint64_t)tot * (w + 1) / kHubWarps));
-    const uint64_t racc = sweep_flat<kHubDepth>(
-        cs, ce, 0, 1,
-        [&](uint32_t i, uint32_t& ib, uint32_t& il) {
-          const uint64_t x = inl[e0 + i];
-          ib = (uint32_t)(x >> 32);
-          il = (uint32_t)x;
-        },
-        [&](uint32_t k) -> uint64_t { return g.bent[k]; },
-        [&](uint64_t e) -> uint32_t {
-          const uint32_t o = (uint32_t)(e >> 32) - bmin;
-          return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
-        });
+    const uint64_t racc = hub_sweep(g, inl + e0, cs, ce, direct, map, bmin, bmax, logb, runs[w]);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -933,8 +1024,8 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
       __syncthreads();
     }
   }
-  // Phase 2: hubs whose span fits a warp's slice of the map, one warp per
-  // piece, largest hubs first.
+  // Phase 2: hubs whose row fits a warp's slice of the map, one warp per
+  // piece, in wave order.
   uint32_t* wmap = map + w * kHubWarpSpan;
   for (;;) {
     uint32_t t0 = 0;
@@ -942,33 +1033,31 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
     const uint32_t t = __shfl_sync(kFull, t0, 0);
     if (t >= wlen) break;
     const unsigned long long t_start = block_ns ? cycles() : 0ull;
-    const uint64_t pc = hub_pieces[len + wlen - 1 - t];
+    const uint64_t pc = hub_pieces[len + t];
     const uint32_t v = (uint32_t)(pc >> 32);
     const uint32_t e0 = in_off[v] + (uint32_t)pc;
     const uint32_t cnt = min(kHubWarpPiece, in_off[v + 1] - e0);
     const uint64_t a = g.rp[v], b = g.rp[v + 1];
     const uint32_t bs = rp_blk(a), be = rp_blk(b);
-    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32);
-    const uint32_t span = (uint32_t)(g.bent[be - 1] >> 32) - bmin + 1;  // <= kHubWarpSpan by the schedule
-    for (uint32_t i = lane; i < span; i += 32) wmap[i] = 0u;
-    __syncwarp();
-    for (uint32_t k = bs + lane; k < be; k += 32) {
-      const uint64_t e = g.bent[k];
-      wmap[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+    const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32), bmax = (uint32_t)(g.bent[be - 1] >> 32);
+    const uint32_t span = bmax - bmin + 1;
+    const bool direct = span <= kHubWarpSpan;  // else be - bs <= kHubWarpHash (schedule)
+    const int logb = table_logb(be - bs);
+    if (direct) {
+      for (uint32_t i = lane; i < span; i += 32) wmap[i] = 0u;
+      __syncwarp();
+      for (uint32_t k = bs + lane; k < be; k += 32) {
+        const uint64_t e = g.bent[k];
+        wmap[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+      }
+    } else {
+      uint64_t* wtbl = reinterpret_cast<uint64_t*>(wmap);
+      table_clear(wtbl, logb, lane, 32);
+      __syncwarp();
+      table_insert(wtbl, logb, g.bent, bs, be, lane, 32);
     }
     __syncwarp();
-    const uint64_t racc = sweep_flat<kHubDepth>(
-        0, cnt, 0, 1,
-        [&](uint32_t i, uint32_t& ib, uint32_t& il) {
-          const uint64_t x = inl[e0 + i];
-          ib = (uint32_t)(x >> 32);
-          il = (uint32_t)x;
-        },
-        [&](uint32_t k) -> uint64_t { return g.bent[k]; },
-        [&](uint64_t e) -> uint32_t {
-          const uint32_t o = (uint32_t)(e >> 32) - bmin;
-          return o < span ? (uint32_t)__popc((uint32_t)e & wmap[o]) : 0u;
-        });
+    const uint64_t racc = hub_sweep(g, inl + e0, 0, cnt, direct, wmap, bmin, bmax, logb, runs[w]);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -1232,11 +1321,13 @@ template <int Mode>
 __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of, const uint64_t* __restrict__ vinfo,
                             unsigned long long* __restrict__ save, uint32_t* __restrict__ eflag,
                             uint32_t* __restrict__ in_cnt, const uint32_t* __restrict__ in_off,
-                            uint64_t* __restrict__ inl, uint32_t* __restrict__ inrow) {
+                            uint64_t* __restrict__ inl, uint32_t* __restrict__ inrow,
+                            const uint32_t* __restrict__ rows) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < g.n; u += nwarps) {
+  const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
+  for (uint32_t u = u0 + warp; u < u1; u += nwarps) {
     if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
     const uint64_t a = g.rp[u], b = g.rp[u + 1];
     const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), nbu = rp_blk(b) - bs;
@@ -1260,12 +1351,15 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
         const uint64_t vi = vinfo[v];
         nbv = (uint32_t)vi;
         span = (uint32_t)(vi >> 32);
-        hub = nbv > 0 && span <= kHubMaxSpan && tail < nbv;
+        hub = nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
       }
       if (Mode == 0) {
         if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
       } else if (Mode == 1) {
-        hub = hub && save[v] >= (unsigned long long)(span / 4 + nbv);
+        // Staging cost: the direct map's span / 4 vector stores, or a hash's
+        // 2 nb slots cleared, plus nb inserts.
+        hub = hub && save[v] >= (span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
+                                                     : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin);
         const uint32_t bits = __ballot_sync(kFull, hub);
         if (lane == 0 && bits) {
           const uint32_t sh = c & 31;
@@ -1295,7 +1389,11 @@ __global__ void k_hub_piece_count(const uint32_t* __restrict__ in_off, const uin
   uint32_t c = 0, wc = 0;
   if (v < n) {
     const uint32_t k = in_off[v + 1] - in_off[v];
-    if ((uint32_t)(vinfo[v] >> 32) <= kHubWarpSpan)
+    const uint32_t span = (uint32_t)(vinfo[v] >> 32), nb = (uint32_t)vinfo[v];
+    // The warp stages the row when its direct map fits the warp's slice, or,
+    // for a row too wide for the CTA's direct map, when its hash does.
+    const bool warp = span <= kHubWarpSpan || (span > kHubMaxSpan && nb <= kHubWarpHash);
+    if (warp)
       wc = (k + kHubWarpPiece - 1) / kHubWarpPiece;
     else
       c = (k + kHubPiece - 1) / kHubPiece;
@@ -1322,6 +1420,69 @@ __global__ void k_hub_piece_scatter(const uint32_t* __restrict__ pos, uint32_t n
 
 __global__ void k_hub_total(const uint32_t* __restrict__ in_off, uint32_t n, uint32_t* __restrict__ piece_off) {
   piece_off[TRIBIT_NUM_VARIANTS + 4] = in_off[n];
+}
+
+// Waves: kHubWaves ranges of rows with equal shares of the bit-row array.
+// wave_lo[w] = first row whose bit row starts at or after w / kHubWaves of
+// it (wave_lo[kHubWaves] = n). The in-lists are filled one wave of rows at a
+// time, so each hub's in-list is ordered by wave, and the hub pieces are then
+// ordered by the wave of their first tail: the CTAs working at one time walk
+// the tails of rows of one wave, whose bit rows fit the L2.
+__global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo) {
+  const uint32_t w = threadIdx.x;
+  if (w > kHubWaves) return;
+  const uint64_t nb = rp_blk(g.rp[g.n]);
+  const uint64_t target = nb * w / kHubWaves;
+  uint32_t lo = 0, hi = g.n;  // first u with brow_ptr[u] >= target
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (rp_blk(g.rp[mid]) < target)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  wave_lo[w] = w == kHubWaves ? g.n : lo;
+}
+
+__device__ __forceinline__ uint32_t wave_of(const uint32_t* __restrict__ wave_lo, uint32_t u) {
+  uint32_t w = 0;
+#pragma unroll
+  for (uint32_t st = kHubWaves / 2; st >= 1; st >>= 1)
+    if (w + st < kHubWaves && wave_lo[w + st] <= u) w += st;
+  return w;
+}
+
+// Counting sort of the hub pieces by the wave of their first tail, within
+// each list (CTA pieces [0, Pc), warp pieces [Pc, P)). cnt: 2 kHubWaves.
+__global__ void k_piece_waves(const uint64_t* __restrict__ pieces, const uint32_t* __restrict__ piece_off,
+                              const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ inrow,
+                              const uint32_t* __restrict__ wave_lo, uint32_t* __restrict__ cnt,
+                              uint8_t* __restrict__ wave) {
+  const uint32_t pc_n = piece_off[TRIBIT_NUM_VARIANTS + 2], all = piece_off[TRIBIT_NUM_VARIANTS + 3];
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < all; p += gridDim.x * blockDim.x) {
+    const uint64_t pc = pieces[p];
+    const uint32_t w = wave_of(wave_lo, inrow[in_off[pc >> 32] + (uint32_t)pc]);
+    wave[p] = (uint8_t)w;
+    atomicAdd(&cnt[(p < pc_n ? 0 : kHubWaves) + w], 1u);
+  }
+}
+
+__global__ void k_wave_scan(uint32_t* __restrict__ cnt, const uint32_t* __restrict__ piece_off) {
+  uint32_t run = 0;
+  for (uint32_t i = 0; i < 2 * kHubWaves; ++i) {
+    if (i == kHubWaves) run = piece_off[TRIBIT_NUM_VARIANTS + 2];  // warp pieces follow the CTA pieces
+    const uint32_t c = cnt[i];
+    cnt[i] = run;
+    run += c;
+  }
+}
+
+__global__ void k_piece_wave_scatter(const uint64_t* __restrict__ pieces, const uint32_t* __restrict__ piece_off,
+                                     const uint8_t* __restrict__ wave, uint32_t* __restrict__ pos,
+                                     uint64_t* __restrict__ out) {
+  const uint32_t pc_n = piece_off[TRIBIT_NUM_VARIANTS + 2], all = piece_off[TRIBIT_NUM_VARIANTS + 3];
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < all; p += gridDim.x * blockDim.x)
+    out[atomicAdd(&pos[(p < pc_n ? 0 : kHubWaves) + wave[p]], 1u)] = pieces[p];
 }
 
 }  // namespace
@@ -1354,6 +1515,10 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.inl = ar.take<uint64_t>(E + 1);
     s.inrow = ar.take<uint32_t>(E + 1);
     s.hub_pieces = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
+    s.hub_pieces2 = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
+    s.piece_wave = ar.take<uint8_t>(2 * n + E / kHubWarpPiece + 64);
+    s.wave_lo = ar.take<uint32_t>(kHubWaves + 1);
+    s.wave_cnt = ar.take<uint32_t>(2 * kHubWaves);
     s.hub_pos = ar.take<uint32_t>(2 * (n + 1));
     s.hub_scan_tmp = take_scan_temp<uint32_t>(ar, 2 * (n + 1));
   }
@@ -1376,22 +1541,34 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(s.eflag, 0, (s.eflag_words) * sizeof(uint32_t), st));
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
   k_hub_edges<0><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow);
+                                           s.inrow, nullptr);
   TB_LAUNCH_CHECK();
   k_hub_edges<1><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow);
+                                           s.inrow, nullptr);
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.in_cnt, s.in_off, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
-  k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow);
+  k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo);
   TB_LAUNCH_CHECK();
+  for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
+    k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                             s.inrow, s.wave_lo + w);
+    TB_LAUNCH_CHECK();
+  }
   k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, s.vinfo, (uint32_t)n, s.hub_pos);
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.hub_pos, s.hub_pos, 2 * (n + 1), true, OpSum{}, 0u, s.hub_scan_tmp, st);
-  k_hub_piece_scatter<<<vblocks, 256, 0, st>>>(s.hub_pos, (uint32_t)n, s.hub_pieces, s.piece_off);
+  k_hub_piece_scatter<<<vblocks, 256, 0, st>>>(s.hub_pos, (uint32_t)n, s.hub_pieces2, s.piece_off);
   TB_LAUNCH_CHECK();
   k_hub_total<<<1, 1, 0, st>>>(s.in_off, (uint32_t)n, s.piece_off);
+  TB_LAUNCH_CHECK();
+  TB_CUDA(cudaMemsetAsync(s.wave_cnt, 0, 2 * kHubWaves * sizeof(uint32_t), st));
+  k_piece_waves<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.in_off, s.inrow, s.wave_lo, s.wave_cnt,
+                                          s.piece_wave);
+  TB_LAUNCH_CHECK();
+  k_wave_scan<<<1, 1, 0, st>>>(s.wave_cnt, s.piece_off);
+  TB_LAUNCH_CHECK();
+  k_piece_wave_scatter<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.piece_wave, s.wave_cnt, s.hub_pieces);
   TB_LAUNCH_CHECK();
   s.hubs_active = true;
 }

@@ -53,6 +53,10 @@ struct Schedule {
   uint64_t* inl = nullptr;         // device: (first block of u's tail << 32) | tail length
   uint32_t* inrow = nullptr;       // device: u of each in-list entry
   uint64_t* hub_pieces = nullptr;  // device: (v << 32) | first in-list entry; CTA pieces, then warp pieces
+  uint64_t* hub_pieces2 = nullptr; // device: the pieces in hub order, before the wave sort
+  uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail
+  uint32_t* wave_lo = nullptr;     // device: first row of each wave, then n
+  uint32_t* wave_cnt = nullptr;    // device: pieces per (list, wave), scanned to positions
   uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
   uint32_t* hub_scan_tmp = nullptr;
   bool hubs = true;                // build the hub lists for merge row blocks
