@@ -193,7 +193,9 @@ __device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, uint32_
 // memory (wsm), each lane finds the owner of its first item once by binary
 // search and then only advances it (items of a lane only grow), so a long
 // list costs one shared-memory compare per item instead of a 5-step search.
-template <int Depth, class Desc, class Load, class Probe>
+// Chunks whose lists average under MinAvg items keep the shuffle search
+// (measured: 8 for hub tails, 32 for bit rows).
+template <int Depth, uint32_t MinAvg, class Desc, class Load, class Probe>
 __device__ __forceinline__ uint64_t sweep_runs(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
                                                const Desc& desc, const Load& load, const Probe& probe,
                                                uint32_t* wsm) {
@@ -205,6 +207,31 @@ __device__ __forceinline__ uint64_t sweep_runs(uint32_t cs, uint32_t ce, uint32_
     if (j < ce) desc(j, ib, il);
     const uint32_t incl = warp_inclusive_sum(il);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (total < 32 * MinAvg) {
+      // Short lists: a lane would cross several lists per step; the shuffle
+      // search of sweep_flat is cheaper here.
+      const uint32_t offs = ib - (incl - il);
+      uint32_t racc = 0;
+      for (uint32_t base = 0; base < total; base += 32 * Depth) {
+        uint64_t x[Depth];
+#pragma unroll
+        for (int r = 0; r < Depth; ++r) {
+          const uint32_t t = base + 32 * r + lane;
+          uint32_t so = 0;
+#pragma unroll
+          for (uint32_t st = 16; st >= 1; st >>= 1) {
+            const uint32_t y = __shfl_sync(kFull, incl, so + st - 1);
+            if (y <= t) so += st;
+          }
+          const uint32_t o = __shfl_sync(kFull, offs, so);
+          x[r] = t < total ? load(o + t) : 0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < Depth; ++r) racc += probe(x[r]);
+      }
+      acc += racc;
+      continue;
+    }
     __syncwarp();
     wsm[lane] = incl;
     wsm[32 + lane] = ib - (incl - il);  // item t of the chunk, owned by slot s, is item off_s + t
@@ -270,7 +297,7 @@ constexpr int kBitsDepth = TB_BITS_DEPTH;
 template <class Probe>
 __device__ __forceinline__ uint64_t sweep_bits(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
                                                uint32_t step, const Probe& probe, uint32_t* wsm) {
-  return sweep_runs<kBitsDepth>(
+  return sweep_runs<kBitsDepth, 32>(
       cs, ce, chunk0, step,
       [&](uint32_t j, uint32_t& ib, uint32_t& il) {
         if (edge_to_hub(g, j)) return;
@@ -918,13 +945,13 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   auto load = [&](uint32_t k) -> uint64_t { return g.bent[k]; };
   if (direct) {
     const uint32_t span = bmax - bmin + 1;
-    return sweep_runs<kHubDepth>(cs, ce, 0, 1, desc, load, [&](uint64_t e) -> uint32_t {
+    return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, [&](uint64_t e) -> uint32_t {
       const uint32_t o = (uint32_t)(e >> 32) - bmin;
       return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
     }, wsm);
   }
   const BitmapProbe probe{reinterpret_cast<const uint64_t*>(map), logb, bmin, bmax};
-  return sweep_runs<kHubDepth>(cs, ce, 0, 1, desc, load, probe, wsm);
+  return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
 }
 
 __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
