@@ -47,6 +47,10 @@ WORKLOADS = {
     "rmat20": {"gen": "rmat", "scale": 20, "edge_factor": 16, "seed": 20},
     "chung_lu": {"gen": "chung_lu", "n": 7115, "n_entries": 115300, "beta": 2.0, "max_degree": 1000.0, "seed": 1},
     "planted": {"gen": "planted", "communities": 20000, "size": 100, "p_in": 0.3, "inter": 2, "seed": 3},
+    # Dense-tile stress: disjoint cliques on consecutive ids; every vertex has
+    # the same degree, so the degree order keeps each clique contiguous and
+    # every row block fits one bit tile.
+    "cliques": {"gen": "cliques", "count": 512, "size": 512, "seed": 0},
 }
 
 
@@ -59,6 +63,14 @@ def make_graph(tb, spec, rank):
         return s["n"], tb.gen_chung_lu(s["n"], s["n_entries"], s["beta"], s["max_degree"], seed)
     if s["gen"] == "planted":
         return s["communities"] * s["size"], tb.gen_planted(s["communities"], s["size"], s["p_in"], s["inter"], seed)
+    if s["gen"] == "cliques":
+        import numpy as np
+        k, c = s["size"], s["count"]
+        i, j = np.triu_indices(k, 1)
+        base = (np.arange(c, dtype=np.uint64) * np.uint64(k))[:, None]
+        lo = (base + i.astype(np.uint64)[None, :]).ravel()
+        hi = (base + j.astype(np.uint64)[None, :]).ravel()
+        return c * k, (lo << np.uint64(32)) | hi
     raise ValueError(s["gen"])
 
 
@@ -272,6 +284,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
+    ap.add_argument("--tile-engine", default="mma_sync", choices=["mma_sync", "tcgen05"],
+                    help="arithmetic of the bit-tile variant")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -313,6 +327,7 @@ def main():
 
     def timed_counter(mode):
         c = tb.Counter(device=local, dispatch=mode)
+        c.set_tile_engine(args.tile_engine)
         if mode == "learned":
             c.load_model(model_path)
         c.set_stream(stream.cuda_stream)
@@ -403,7 +418,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": args.workload, **spec, "n": n, "entries": int(entries.size), "edges": m,
-                       "triangles": res.triangles, "dispatch": dispatch, "parallelism": f"replicas{world}",
+                       "triangles": res.triangles, "dispatch": dispatch, "tile_engine": args.tile_engine,
+                       "parallelism": f"replicas{world}",
                        "l2": "256 MiB buffer written between timed steps; inputs > L2",
                        "preprocess_ms": prep.preprocess_ms, "gen_s": round(gen_s, 2),
                        "row_blocks_by_variant": dict(zip(tb.VARIANTS, res.row_blocks_by_variant)),

@@ -77,6 +77,10 @@ typedef struct tribit_options {
   uint32_t reserved[8];  /* must be zero */
 } tribit_options;
 
+/* Bit-tile variant: the product's arithmetic. */
+enum { TRIBIT_TILES_MMA_SYNC = 0, /* legacy warp-level mma.sync m16n8k256 b1 AND+POPC */
+       TRIBIT_TILES_TCGEN05 = 1   /* tcgen05.mma kind::i8 on bits unpacked to 0/1, s32 in TMEM */ };
+
 typedef struct tribit_result {
   uint64_t triangles;         /* exact count */
   uint64_t num_nodes;         /* n as given */
@@ -139,6 +143,9 @@ tribit_status tribit_set_tuning(tribit_context* ctx, const tribit_tuning* in);
  * small grid (CTAs/SM x piece width x tile threshold), keeps the fastest
  * (median) and returns it. Counts stay exact under every setting. */
 tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning* best);
+/* Arithmetic of the bit-tile variant (TRIBIT_TILES_*), for later launches;
+ * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_MMA_SYNC. */
+tribit_status tribit_set_tile_engine(tribit_context* ctx, int engine);
 /* Captures the counting launch of the prepared graph (or batch) into a CUDA
  * graph; tribit_launch_count then replays it with one graph launch. Preparing
  * another input or changing the tuning drops the capture. */

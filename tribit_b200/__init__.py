@@ -37,6 +37,7 @@ lib = ctypes.CDLL(LIB_PATH)
 ORDERS = {"degree": 0, "id": 1}
 DISPATCH = {"plain": 0, "learned": 1, "merge": 2, "bitmap": 3, "mma": 4}
 VARIANTS = ("mma", "bitmap", "merge")
+TILE_ENGINES = ("mma_sync", "tcgen05")
 
 _u64 = ctypes.c_uint64
 _u32 = ctypes.c_uint32
@@ -103,6 +104,7 @@ class Tuning(ctypes.Structure):
 _decl("tribit_get_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
 _decl("tribit_set_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
 _decl("tribit_autotune", ctypes.c_int, _p, _u32, ctypes.POINTER(Tuning))
+_decl("tribit_set_tile_engine", ctypes.c_int, _p, ctypes.c_int)
 _decl("tribit_capture_count", ctypes.c_int, _p)
 _decl("tribit_read_batch_counts", ctypes.c_int, _p, _p, _u32)
 _decl("tribit_gen_batch", ctypes.c_int, _u32, _u32, _u32, _u64, _p, _p, _p)
@@ -204,6 +206,10 @@ class Counter:
     def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 1e30):
         t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0)
         _check(lib.tribit_set_tuning(self._h, ctypes.byref(t)), self._h)
+
+    def set_tile_engine(self, engine: str):
+        """Arithmetic of the bit-tile variant: "mma_sync" (b1 AND+POPC) or "tcgen05" (kind::i8)."""
+        _check(lib.tribit_set_tile_engine(self._h, TILE_ENGINES.index(engine)), self._h)
 
     def autotune(self, reps: int = 2) -> Tuning:
         t = Tuning()

@@ -345,6 +345,15 @@ tribit_status tribit_set_tuning(tribit_context* c, const tribit_tuning* t) {
   });
 }
 
+tribit_status tribit_set_tile_engine(tribit_context* c, int engine) {
+  if (!c || (engine != TRIBIT_TILES_MMA_SYNC && engine != TRIBIT_TILES_TCGEN05)) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->tile_engine = engine;
+    c->sched.tile_engine = engine;
+    tb::drop_graph(c);
+  });
+}
+
 tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* best) {
   if (!c || !c->prepared || !best) return TRIBIT_ERR_INVALID_ARGUMENT;
   if (reps == 0) reps = 2;

@@ -788,6 +788,284 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
   if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
+// ---- bit-tile variant on the 5th-generation tensor cores (tcgen05) ----------
+// Same pieces as k_tiles_mma (a row block R whose rows fit one column range of
+// K <= kTileMaxK blocks, and 128 neighbours V[first, first + 128) of it), but
+// the product runs as one tcgen05.mma kind::i8 per 32 columns: the 128
+// neighbours' bits over the range, unpacked to 0/1 bytes, are the A operand
+// (M = 128), the block's 32 rows the B operand (N = 32), both K-major in
+// shared memory without swizzle; D[v][u] = |N+(v) & N+(u)| accumulates in
+// TMEM as s32 (exact: at most K * 32 = 2048 per element). One elected thread
+// issues the MMAs and commits them to an mbarrier that every thread waits on
+// with a bounded wait; each warp then reads its 32 TMEM lanes (rows v) and
+// adds D[v][u] where u has v. The CTA allocates its 32 TMEM columns once and
+// frees them before it exits, also after a failed wait.
+
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTcChunk = 256;                 // K bytes (columns) unpacked per round
+constexpr uint32_t kTcWaitIters = 1u << 22;        // mbarrier polls before giving up
+
+struct TcSmem {
+  uint8_t a[kTileNbrPiece * kTcChunk];             // A: 128 rows x 256 K-bytes, core-matrix layout
+  uint8_t b[32 * kTcChunk];                        // B: 32 rows x 256 K-bytes
+  uint32_t vbits[kTileNbrPiece][kTileMaxK];        // the neighbours' bits over the block's range
+  uint32_t ubits[32][kTileMaxK];                   // the block's rows
+  uint32_t vmask[kTileMaxK];                       // OR of the rows: V
+  uint32_t vpre[kTileMaxK + 1];                    // popcount prefix of vmask
+  uint32_t row_bs[32], row_be[32];
+  unsigned long long mbar;
+  uint32_t tmem;
+  uint32_t lo, K, amask, cnt_v, fail;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
+// matrices, lbo bytes between core matrices along K, sbo along M/N.
+__device__ __forceinline__ uint64_t umma_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((smem_addr(p) >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::i8: D s32, A and B unsigned 8-bit, both
+// K-major, N = 32, M = 128.
+constexpr uint32_t kTcIdesc = (2u << 4) | (0u << 7) | (0u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+// Unpacks 32 bits (LSB = first column) to 32 bytes of 0/1 as two uint4.
+__device__ __forceinline__ void unpack32(uint32_t x, uint4& lo16, uint4& hi16) {
+  auto nib = [](uint32_t v) -> uint32_t { return (v & 0xFu) * 0x00204081u & 0x01010101u; };
+  lo16 = make_uint4(nib(x), nib(x >> 4), nib(x >> 8), nib(x >> 12));
+  hi16 = make_uint4(nib(x >> 16), nib(x >> 20), nib(x >> 24), nib(x >> 28));
+}
+
+// Byte offset of (row, 16-byte K group) in a K-major no-swizzle operand of
+// kTcChunk K-bytes: core matrices of 8 rows x 16 bytes, 128 bytes apart along
+// K (LBO) and 16 * 128 bytes apart along the rows (SBO).
+__device__ __forceinline__ uint32_t tc_off(uint32_t row, uint32_t kgroup) {
+  return (row >> 3) * (kTcChunk / 16) * 128 + kgroup * 128 + (row & 7) * 16;
+}
+
+__device__ __forceinline__ bool tc_wait(unsigned long long* mbar, uint32_t parity) {
+  uint32_t done = 0;
+  for (uint32_t i = 0; i < kTcWaitIters && !done; ++i)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(mbar)), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+
+__global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint64_t* __restrict__ pieces,
+                                                         const uint32_t* __restrict__ piece_off, DeviceStats* stats,
+                                                         unsigned long long* per_graph,
+                                                         unsigned long long* block_ns) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t p0 = piece_off[TRIBIT_VARIANT_MMA], len = piece_off[TRIBIT_VARIANT_MMA + 1] - p0;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&sm.mbar)), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    sm.fail = 0;
+  }
+  if (w == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_addr(&sm.tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = sm.tmem;
+  uint32_t phase = 0;
+  uint64_t acc = 0;
+  __shared__ uint32_t s_t;
+  for (;;) {
+    if (tid == 0) s_t = atomicAdd(&stats->cursor[kCurVariant0 + TRIBIT_VARIANT_MMA], 1u);
+    __syncthreads();
+    const uint32_t t = s_t;
+    if (t >= len || sm.fail) break;
+    const unsigned long long t_start = (block_ns && tid == 0) ? cycles() : 0ull;
+    const uint64_t pc = pieces[p0 + (len - 1 - t)];
+    const uint32_t rb = (uint32_t)(pc >> 32) >> 5, first = (uint32_t)pc;
+    // The block's rows: activity and the column range (warp 0).
+    if (w == 0) {
+      const uint32_t u = rb * 32 + lane;
+      uint32_t bs = 0, be = 0, lo = 0xFFFFFFFFu, hi = 0;
+      bool active = false;
+      if (u < g.n) {
+        const uint64_t a = g.rp[u], b = g.rp[u + 1];
+        bs = rp_blk(a);
+        be = rp_blk(b);
+        active = rp_row(b) - rp_row(a) >= 2 && be - bs <= kWarpMaxBlocks;
+        if (active) {
+          lo = (uint32_t)(g.bent[bs] >> 32);
+          hi = (uint32_t)(g.bent[be - 1] >> 32);
+        }
+      }
+      const uint32_t amask = __ballot_sync(kFull, active);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+      }
+      sm.row_bs[lane] = active ? bs : 0u;
+      sm.row_be[lane] = active ? be : 0u;
+      if (lane == 0) {
+        sm.amask = amask;
+        sm.lo = lo;
+        sm.K = amask ? hi - lo + 1 : 0u;
+      }
+    }
+    __syncthreads();
+    const uint32_t K = sm.K, lo = sm.lo, amask = sm.amask;
+    uint64_t racc = 0;
+    if (K > (uint32_t)kTileMaxK) {
+      // Forced onto a block that fits no tile: its one piece sweeps the rows (warp 0).
+      if (first == 0 && w == 0)
+        racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.vbits), sm.vpre, per_graph);
+    } else if (K > 0) {
+      const uint32_t KW = (K + 7) & ~7u;  // words, whole 256-column chunks
+      for (uint32_t i = tid; i < 32 * kTileMaxK; i += kTcThreads) (&sm.ubits[0][0])[i] = 0u;
+      for (uint32_t i = tid; i < kTileNbrPiece * kTileMaxK; i += kTcThreads) (&sm.vbits[0][0])[i] = 0u;
+      __syncthreads();
+      // The rows' bits: warp w takes rows w, w + 4, ...
+      for (uint32_t r = w; r < 32; r += 4) {
+        if (!((amask >> r) & 1u)) continue;
+        for (uint32_t k = sm.row_bs[r] + lane; k < sm.row_be[r]; k += 32) {
+          const uint64_t e = g.bent[k];
+          sm.ubits[r][(uint32_t)(e >> 32) - lo] = (uint32_t)e;
+        }
+      }
+      __syncthreads();
+      if (tid < (uint32_t)kTileMaxK) {
+        uint32_t m = 0;
+        if (tid < K)
+          for (uint32_t r = 0; r < 32; ++r) m |= sm.ubits[r][tid];
+        sm.vmask[tid] = m;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t run = 0;
+        for (uint32_t i = 0; i < (uint32_t)kTileMaxK; ++i) {
+          sm.vpre[i] = run;
+          run += __popc(sm.vmask[i]);
+        }
+        sm.vpre[kTileMaxK] = run;
+        sm.cnt_v = min(kTileNbrPiece, run > first ? run - first : 0u);
+      }
+      __syncthreads();
+      // Neighbour tid of the piece: the (first + tid)-th set bit of V; its
+      // bits over the range, gathered by this thread.
+      const uint32_t nv = sm.cnt_v;
+      uint32_t vcol = 0xFFFFFFFFu;
+      if (tid < nv) {
+        const uint32_t idx = first + tid;
+        uint32_t wd = 0;
+#pragma unroll
+        for (uint32_t st = 32; st >= 1; st >>= 1)
+          if (wd + st < (uint32_t)kTileMaxK && sm.vpre[wd + st] <= idx) wd += st;
+        uint32_t m = sm.vmask[wd];
+        for (uint32_t q = idx - sm.vpre[wd]; q > 0; --q) m &= m - 1;
+        vcol = wd * 32 + __ffs(m) - 1;
+        const uint32_t v = lo * 32 + vcol;
+        const uint64_t va = g.rp[v], vb = g.rp[v + 1];
+        const uint32_t vbs = rp_blk(va), vn = min(rp_blk(vb) - vbs, K);
+        for (uint32_t k = 0; k < vn; ++k) {
+          const uint64_t e = g.bent[vbs + k];
+          const uint32_t blk = (uint32_t)(e >> 32) - lo;
+          if (blk < K) sm.vbits[tid][blk] = (uint32_t)e;
+        }
+      }
+      __syncthreads();
+      for (uint32_t c = 0; c < KW; c += kTcChunk / 32) {
+        // Unpack this chunk: thread tid row tid of A (8 words = 16 groups of
+        // 16 bytes); B rows by all threads, a quarter row each.
+        for (uint32_t q = 0; q < kTcChunk / 32; ++q) {
+          uint4 x0, x1;
+          unpack32(sm.vbits[tid][c + q], x0, x1);
+          *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q)) = x0;
+          *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q + 1)) = x1;
+        }
+        {
+          const uint32_t r = tid & 31, q0 = (tid >> 5) * 2;
+          for (uint32_t q = q0; q < q0 + 2; ++q) {
+            uint4 x0, x1;
+            unpack32(sm.ubits[r][c + q], x0, x1);
+            *reinterpret_cast<uint4*>(sm.b + tc_off(r, 2 * q)) = x0;
+            *reinterpret_cast<uint4*>(sm.b + tc_off(r, 2 * q + 1)) = x1;
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sbo = (kTcChunk / 16) * 128;
+          for (uint32_t ks = 0; ks < kTcChunk / 32; ++ks) {
+            const uint64_t ad = umma_desc(sm.a + ks * 256, 128, sbo);
+            const uint64_t bd = umma_desc(sm.b + ks * 256, 128, sbo);
+            const uint32_t accum = (c > 0 || ks > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(accum), "r"(0u)
+                : "memory");
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_addr(&sm.mbar))
+                       : "memory");
+        }
+        const bool ok = tc_wait(&sm.mbar, phase);
+        phase ^= 1u;
+        if (!ok) {
+          if (tid == 0) {
+            atomicOr(&stats->err, kErrTimeout);
+            sm.fail = 1;
+          }
+          break;
+        }
+      }
+      __syncthreads();
+      if (!sm.fail) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+              "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]),
+              "=r"(d[15]), "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]),
+              "=r"(d[22]), "=r"(d[23]), "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]),
+              "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+            : "r"(tmem + ((w * 32u) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        // Lane = neighbour v = row 32w + lane of D; column r = row r of the block.
+        if (tid < nv) {
+          uint64_t sum = 0;
+#pragma unroll
+          for (int r = 0; r < 32; ++r)
+            if ((sm.ubits[r][vcol >> 5] >> (vcol & 31)) & 1u) sum += d[r];
+          racc += sum;
+          if (per_graph && sum) atomicAdd(&per_graph[g.graph_of_rank[lo * 32 + vcol]], (unsigned long long)sum);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      }
+    }
+    acc += racc;
+    __syncthreads();
+    if (block_ns && tid == 0) atomicAdd(&block_ns[rb], (cycles() - t_start) * (kTcThreads / 32));
+  }
+  __syncthreads();
+  // After a failed wait, give the outstanding MMAs one more bounded wait
+  // before their accumulator columns are freed.
+  if (sm.fail) tc_wait(&sm.mbar, phase ^ 1u);
+  __syncthreads();
+  if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+  acc = warp_sum(acc);
+  if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+}
+
 // ---- CTA-per-row pass for rows deferred by the warp kernels ---------------
 
 __device__ __forceinline__ uint64_t block_sum_u64(uint64_t v) {
@@ -1654,6 +1932,7 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
                                  (int)(sizeof(uint64_t) << kCtaLogSlots)));
     TB_CUDA(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kTileWarps * sizeof(TileSmem))));
+    TB_CUDA(cudaFuncSetAttribute(k_tiles_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
     attr_done = true;
   }
   const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
@@ -1670,8 +1949,12 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
   k_pieces_warp<TRIBIT_VARIANT_BITMAP><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(
       g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy, s.piece_width);
   TB_LAUNCH_CHECK();
-  k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
-      g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns);
+  if (s.tile_engine == TRIBIT_TILES_TCGEN05)
+    k_tiles_tc<<<(unsigned)(sms * 2), kTcThreads, sizeof(TcSmem), st>>>(g, s.pieces, s.piece_off, stats, per_graph,
+                                                                         cfg.block_ns);
+  else
+    k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
+        g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   k_pieces_warp<TRIBIT_VARIANT_MERGE><<<warp_grid, kWarpsPerCta * 32, 0, st>>>(g, s.pieces, s.piece_off, stats, ovf_cta,
                                                                                per_graph, cfg.block_ns, nullptr,
@@ -1686,7 +1969,7 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
                                                                      s.inrow, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   if (cfg.variant_stop) TB_CUDA(cudaEventRecord(cfg.variant_stop, st));
-  info.ctas = 2ull * warp_grid + (7ull + kHubCtasPerSm) * sms;
+  info.ctas = 2ull * warp_grid + (2ull + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? 2ull : 5ull) + kHubCtasPerSm) * sms;
   info.kernels = 6;
   return info;
 }

@@ -342,6 +342,7 @@ void apply_dispatch(tribit_context* c, cudaStream_t st) {
   const int mode = c->opts.dispatch;
   c->sched.piece_width = c->piece_width;
   c->sched.tile_min_nnz = c->tile_min_nnz;
+  c->sched.tile_engine = c->tile_engine;
   c->sched.hubs = mode == TRIBIT_DISPATCH_LEARNED || mode == TRIBIT_DISPATCH_MERGE;  // only merge blocks use them
   drop_graph(c);
   if (mode == TRIBIT_DISPATCH_LEARNED) {
