@@ -284,7 +284,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
-    ap.add_argument("--tile-engine", default="mma_sync", choices=["mma_sync", "tcgen05"],
+    ap.add_argument("--tile-engine", default="tcgen05", choices=["mma_sync", "tcgen05"],
                     help="arithmetic of the bit-tile variant")
     args = ap.parse_args()
     if args.warmup < 3:

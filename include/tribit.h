@@ -132,8 +132,8 @@ tribit_status tribit_read_count(tribit_context* ctx, tribit_result* out);
 typedef struct tribit_tuning {
   int ctas_per_sm;      /* CTAs per SM of the warp-per-piece kernels; 0 = default (6) */
   uint32_t piece_width; /* neighbours per work piece: a multiple of 32, >= 32 (default 64) */
-  float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles
-                           (default 1e30: off; the autotuner tries 64) */
+  float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles, which
+                           also need 1/8 of the tile's cells set (default 64; 1e30 = off) */
   float count_ms;       /* tribit_autotune: measured counting time of this setting */
 } tribit_tuning;
 tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);
@@ -144,7 +144,7 @@ tribit_status tribit_set_tuning(tribit_context* ctx, const tribit_tuning* in);
  * (median) and returns it. Counts stay exact under every setting. */
 tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning* best);
 /* Arithmetic of the bit-tile variant (TRIBIT_TILES_*), for later launches;
- * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_MMA_SYNC. */
+ * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_TCGEN05. */
 tribit_status tribit_set_tile_engine(tribit_context* ctx, int engine);
 /* Captures the counting launch of the prepared graph (or batch) into a CUDA
  * graph; tribit_launch_count then replays it with one graph launch. Preparing

@@ -203,7 +203,7 @@ class Counter:
         _check(lib.tribit_get_tuning(self._h, ctypes.byref(t)), self._h)
         return t
 
-    def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 1e30):
+    def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 64.0):
         t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0)
         _check(lib.tribit_set_tuning(self._h, ctypes.byref(t)), self._h)
 

@@ -29,8 +29,8 @@ struct tribit_context {
   // Tuned launch parameters (tribit_set_tuning / tribit_autotune).
   int ctas_per_sm = 0;
   uint32_t piece_width = 64;
-  int tile_engine = TRIBIT_TILES_MMA_SYNC;
-  float tile_min_nnz = 1e30f;  // bit tiles off until tuned on (they lost on every measured workload)
+  int tile_engine = TRIBIT_TILES_TCGEN05;  // measured faster than mma.sync on dense tiles
+  float tile_min_nnz = 64.f;
   uint32_t num_graphs = 0;             // batch size of the prepared input (0: single graph)
   cudaGraph_t graph = nullptr;         // captured counting launch (tribit_capture_count)
   cudaGraphExec_t graph_exec = nullptr;

@@ -577,6 +577,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
 // v_j. Each neighbour's row is read once per row block instead of once per
 // edge. Row blocks that do not fit fall back to the bitmap sweep in place.
 
+constexpr float kTileMinDensityInv = 8.f;      // plain rule: tiles need 1/8 of their cells set
 constexpr int kTileStride = kTileMaxK + 4;      // padded: fragment loads hit 32 distinct banks
 constexpr int kTileWarps = 4;
 constexpr uint32_t kTileNbrPiece = 128;         // neighbours of V per tile piece (16 groups of 8)
@@ -1463,10 +1464,13 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
       f[14] = nnz > 0 ? log2f(1.f + wb / nnz) : 0.f;
       f[15] = log2f(1.f + sq);
       // Plain dispatcher: fixed thresholds. Bit tiles where the block's rows
-      // share one narrow column range and have enough edges to share
-      // neighbours; the bitmap sweep everywhere else.
+      // share one narrow column range and are dense in it (at least 1/8 of
+      // the 32 x 32 * span cells set, and tile_min_nnz edges): on disjoint
+      // cliques tiles beat the sweeps, on sparse small graphs (1-2 % dense)
+      // they lose. The bitmap sweep everywhere else.
       uint8_t var = TRIBIT_VARIANT_BITMAP;
-      if (span > 0.f && span <= (float)kTileMaxK && nnz >= tile_min_nnz) var = TRIBIT_VARIANT_MMA;
+      if (span > 0.f && span <= (float)kTileMaxK && nnz >= tile_min_nnz && nnz >= span * (1024.f / kTileMinDensityInv))
+        var = TRIBIT_VARIANT_MMA;
       if (mode == TRIBIT_DISPATCH_BITMAP) var = TRIBIT_VARIANT_BITMAP;
       if (mode == TRIBIT_DISPATCH_MERGE) var = TRIBIT_VARIANT_MERGE;
       if (mode == TRIBIT_DISPATCH_MMA) var = TRIBIT_VARIANT_MMA;

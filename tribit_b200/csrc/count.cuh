@@ -62,8 +62,8 @@ struct Schedule {
   bool hubs = true;                // build the hub lists for merge row blocks
   bool hubs_active = false;        // set by build_pieces
   uint32_t piece_width = 64;       // neighbours per piece (tuned)
-  float tile_min_nnz = 1e30f;      // plain dispatcher: fewest edges for a bit-tile row block (tuned)
-  int tile_engine = TRIBIT_TILES_MMA_SYNC;  // bit-tile product: b1 mma.sync or tcgen05 kind::i8
+  float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
+  int tile_engine = TRIBIT_TILES_TCGEN05;  // bit-tile product: tcgen05 kind::i8 or b1 mma.sync
   const void* model = nullptr;     // device MLP parameters for learned dispatch
 };
 

@@ -43,10 +43,22 @@ def training_graphs(quick: bool):
     def batch(g, seed):
         return lambda: ("batch", *tb.gen_batch(g, seed=seed))
 
+    def cliques(count, size):
+        # Dense tiles: disjoint cliques on consecutive ids (the planted graph's
+        # random ids leave no tile dense).
+        def make():
+            i, j = np.triu_indices(size, 1)
+            base = (np.arange(count, dtype=np.uint64) * np.uint64(size))[:, None]
+            lo = (base + i.astype(np.uint64)[None, :]).ravel()
+            hi = (base + j.astype(np.uint64)[None, :]).ravel()
+            return "graph", count * size, (lo << np.uint64(32)) | hi
+        return make
+
     if quick:
-        return [("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(4000, 103)), ("batch_s101", batch(64, 101))]
+        return [("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(4000, 103)), ("batch_s101", batch(64, 101)),
+                ("cliques_32x256", cliques(32, 256))]
     return [("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)), ("planted_s103", planted(20000, 103)),
-            ("batch_s101", batch(1024, 101))]
+            ("batch_s101", batch(1024, 101)), ("cliques_96x384", cliques(96, 384))]
 
 
 def holdout_graph(quick: bool):
@@ -92,7 +104,7 @@ def plain_choice(x):
     nnz = np.exp2(x[:, 1]) - 1
     span = np.exp2(x[:, 13]) - 1
     choice = np.full(x.shape[0], tb.VARIANTS.index("bitmap"))
-    mma = (span > 0.5) & (span <= 64.5) & (nnz >= 63.5)
+    mma = (span > 0.5) & (span <= 64.5) & (nnz >= 63.5) & (nnz >= span * 128.0 - 0.5)
     choice[mma] = tb.VARIANTS.index("mma")
     return choice
 
