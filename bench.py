@@ -96,14 +96,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(workload):
-    """Per-launch DRAM bytes of the counting kernels from the committed ncu summary."""
+def profiled_traffic(workload, dispatch):
+    """Per-launch DRAM bytes of the counting kernels from the committed ncu summary
+    (lines: workload, bytes, dispatch)."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == workload:
+        if len(parts) >= 3 and parts[0] == workload and parts[2] == dispatch:
             try:
                 return float(parts[1])
             except ValueError:
@@ -398,7 +399,7 @@ def main():
     peak, peak_kind = measured_peaks()
     b_alg = 4 * (n + 1) + 4 * m
     achieved = b_alg / (ms_per_step / 1e3) / 1e9
-    traffic = profiled_traffic(args.workload)
+    traffic = profiled_traffic(args.workload, dispatch)
 
     batch = None
     if not args.no_batch:
