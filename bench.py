@@ -429,7 +429,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
-                         "algorithmic_bytes": b_alg},
+                         "algorithmic_bytes": b_alg,
+                         # measured DRAM bytes of a launch (ncu, committed) over this run's launch time
+                         "traffic_gbs": traffic / (ms_per_step / 1e3) / 1e9 if traffic else None,
+                         "traffic_frac": traffic / (ms_per_step / 1e3) / 1e9 / peak if traffic else None},
             "cpu_baseline": cpu,
             "e2e": {"value": job_edges / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
                     "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3},

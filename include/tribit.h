@@ -146,6 +146,11 @@ tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning*
 /* Arithmetic of the bit-tile variant (TRIBIT_TILES_*), for later launches;
  * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_TCGEN05. */
 tribit_status tribit_set_tile_engine(tribit_context* ctx, int engine);
+/* Failure-detection test: one counting launch of the prepared graph in which
+ * the tcgen05 tile kernel issues no MMA, so its bounded mbarrier wait runs out
+ * after max_polls polls; the kernel frees its TMEM and returns, and
+ * tribit_read_count then reports TRIBIT_ERR_TIMEOUT. Preparing again clears it. */
+tribit_status tribit_test_tile_timeout(tribit_context* ctx, uint32_t max_polls);
 /* Captures the counting launch of the prepared graph (or batch) into a CUDA
  * graph; tribit_launch_count then replays it with one graph launch. Preparing
  * another input or changing the tuning drops the capture. */

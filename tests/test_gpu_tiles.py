@@ -67,3 +67,22 @@ def test_plain_rule_with_tiles_on_and_tcgen05():
 def test_unknown_tile_engine_is_rejected():
     with tb.Counter() as c:
         assert tb.lib.tribit_set_tile_engine(c._h, 7) == 1  # TRIBIT_ERR_INVALID_ARGUMENT
+
+
+def test_tile_wait_times_out_and_the_context_recovers():
+    # The tcgen05 tile kernel's mbarrier wait is bounded: with its MMAs never
+    # committed it gives up, frees its TMEM and the host reads TRIBIT_ERR_TIMEOUT;
+    # the context and the GPU stay usable.
+    import torch
+    n, e = cliques_on_consecutive_ids([256] * 8)
+    d = torch.from_numpy(e.view(np.int64)).cuda()
+    with tb.Counter(dispatch="mma") as c:
+        c.set_tile_engine("tcgen05")
+        c.prepare_device(d.data_ptr(), d.numel(), n)
+        assert tb.lib.tribit_test_tile_timeout(c._h, 1024) == 0
+        with pytest.raises(tb.TribitError) as ex:
+            c.read_count()
+        assert ex.value.status == 10  # TRIBIT_ERR_TIMEOUT
+        c.prepare_device(d.data_ptr(), d.numel(), n)
+        c.launch_count()
+        assert c.read_count().triangles == 8 * comb(256)

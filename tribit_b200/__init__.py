@@ -105,6 +105,7 @@ _decl("tribit_get_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
 _decl("tribit_set_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
 _decl("tribit_autotune", ctypes.c_int, _p, _u32, ctypes.POINTER(Tuning))
 _decl("tribit_set_tile_engine", ctypes.c_int, _p, ctypes.c_int)
+_decl("tribit_test_tile_timeout", ctypes.c_int, _p, _u32)
 _decl("tribit_capture_count", ctypes.c_int, _p)
 _decl("tribit_read_batch_counts", ctypes.c_int, _p, _p, _u32)
 _decl("tribit_gen_batch", ctypes.c_int, _u32, _u32, _u32, _u64, _p, _p, _p)

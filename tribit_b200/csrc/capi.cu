@@ -354,6 +354,20 @@ tribit_status tribit_set_tile_engine(tribit_context* c, int engine) {
   });
 }
 
+tribit_status tribit_test_tile_timeout(tribit_context* c, uint32_t max_polls) {
+  if (!c || !c->prepared || max_polls == 0) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    tb::drop_graph(c);
+    tb::CountConfig cfg;
+    cfg.num_sms = c->num_sms;
+    cfg.ctas_per_sm = c->ctas_per_sm;
+    cfg.tile_wait_polls = max_polls;
+    cfg.tile_test_no_commit = 1;
+    c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
+  });
+}
+
 tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* best) {
   if (!c || !c->prepared || !best) return TRIBIT_ERR_INVALID_ARGUMENT;
   if (reps == 0) reps = 2;

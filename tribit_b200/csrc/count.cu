@@ -804,7 +804,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
 
 constexpr int kTcThreads = 128;
 constexpr uint32_t kTcChunk = 256;                 // K bytes (columns) unpacked per round
-constexpr uint32_t kTcWaitIters = 1u << 22;        // mbarrier polls before giving up
+
 
 struct TcSmem {
   uint8_t a[kTileNbrPiece * kTcChunk];             // A: 128 rows x 256 K-bytes, core-matrix layout
@@ -846,9 +846,9 @@ __device__ __forceinline__ uint32_t tc_off(uint32_t row, uint32_t kgroup) {
   return (row >> 3) * (kTcChunk / 16) * 128 + kgroup * 128 + (row & 7) * 16;
 }
 
-__device__ __forceinline__ bool tc_wait(unsigned long long* mbar, uint32_t parity) {
+__device__ __forceinline__ bool tc_wait(unsigned long long* mbar, uint32_t parity, uint32_t max_polls) {
   uint32_t done = 0;
-  for (uint32_t i = 0; i < kTcWaitIters && !done; ++i)
+  for (uint32_t i = 0; i < max_polls && !done; ++i)
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
@@ -857,10 +857,14 @@ __device__ __forceinline__ bool tc_wait(unsigned long long* mbar, uint32_t parit
   return done != 0;
 }
 
+// test_no_commit (failure-detection test only): the MMAs are neither issued
+// nor committed, so the first wait runs out after max_polls and the kernel
+// takes its error path.
 __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint64_t* __restrict__ pieces,
                                                          const uint32_t* __restrict__ piece_off, DeviceStats* stats,
                                                          unsigned long long* per_graph,
-                                                         unsigned long long* block_ns) {
+                                                         unsigned long long* block_ns, uint32_t max_polls,
+                                                         int test_no_commit) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -1000,7 +1004,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !test_no_commit) {
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t sbo = (kTcChunk / 16) * 128;
           for (uint32_t ks = 0; ks < kTcChunk / 32; ++ks) {
@@ -1017,7 +1021,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
                            smem_addr(&sm.mbar))
                        : "memory");
         }
-        const bool ok = tc_wait(&sm.mbar, phase);
+        const bool ok = tc_wait(&sm.mbar, phase, max_polls);
         phase ^= 1u;
         if (!ok) {
           if (tid == 0) {
@@ -1060,7 +1064,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
   __syncthreads();
   // After a failed wait, give the outstanding MMAs one more bounded wait
   // before their accumulator columns are freed.
-  if (sm.fail) tc_wait(&sm.mbar, phase ^ 1u);
+  if (sm.fail) tc_wait(&sm.mbar, phase ^ 1u, max_polls);
   __syncthreads();
   if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
   acc = warp_sum(acc);
@@ -1955,7 +1959,8 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
   TB_LAUNCH_CHECK();
   if (s.tile_engine == TRIBIT_TILES_TCGEN05)
     k_tiles_tc<<<(unsigned)(sms * 2), kTcThreads, sizeof(TcSmem), st>>>(g, s.pieces, s.piece_off, stats, per_graph,
-                                                                         cfg.block_ns);
+                                                                         cfg.block_ns, cfg.tile_wait_polls,
+                                                                         cfg.tile_test_no_commit);
   else
     k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
         g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns);

@@ -74,6 +74,8 @@ struct CountConfig {
   unsigned long long* block_ns = nullptr;  // optional: per-row-block warp-cycles (SM cycles x warps busy)
   cudaEvent_t variant_start = nullptr;     // optional (timing mode): these events bracket
   cudaEvent_t variant_stop = nullptr;      // all counting kernels
+  uint32_t tile_wait_polls = 1u << 22;     // tcgen05 tiles: mbarrier polls before a wait gives up
+  int tile_test_no_commit = 0;             // failure-detection test: tile MMAs never committed
 };
 
 // hubs: also take the hub-pass arrays (about 13 bytes per entry).
