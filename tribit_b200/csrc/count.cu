@@ -32,6 +32,7 @@ enum { kCurVariant0 = 0, kCurHubWarp = 3, kCurCta = 4, kCurGlobal = 5, kCurHeavy
 // memory, the row's per-neighbour item prefix in the second 16 KiB.
 constexpr uint32_t kHeavyMaxBlocks = kWarpsPerCta * kWarpSlots / 4;
 constexpr uint32_t kHeavyMaxDeg = kWarpsPerCta * kWarpSlots - 1;
+constexpr uint32_t kHeavyMaxSpan = kWarpsPerCta * kWarpSlots;  // direct-mapped row: 16 KiB of masks
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 enum { kOvfCta = 0, kOvfGlobal = 1 };
 
@@ -446,15 +447,32 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         __syncthreads();
         continue;
       }
+      // u's row: a direct-mapped mask array over its block span when that
+      // fits the table's 16 KiB (the top-ranked rows), else the bucketed hash.
+      const uint32_t bmin = (uint32_t)(g.bent[bs] >> 32), bmax = (uint32_t)(g.bent[be - 1] >> 32);
+      const uint32_t span = bmax - bmin + 1;
+      const bool direct = span <= kHeavyMaxSpan;
+      uint32_t* cmap = reinterpret_cast<uint32_t*>(ctbl);
       const int logb = table_logb(nb);
-      table_clear(ctbl, logb, threadIdx.x, blockDim.x);
+      if (direct) {
+        for (uint32_t i = threadIdx.x; i < span; i += blockDim.x) cmap[i] = 0u;
+      } else {
+        table_clear(ctbl, logb, threadIdx.x, blockDim.x);
+      }
       // Item prefix: pre[j] = bit blocks of the neighbours before j, pre[d] = all.
       for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
         const uint32_t v = g.col[rs + j];
         pre[j] = edge_to_hub(g, rs + j) ? 0u : rp_blk(g.rp[v + 1]) - rp_blk(g.rp[v]);
       }
       __syncthreads();
-      table_insert(ctbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
+      if (direct) {
+        for (uint32_t k = bs + threadIdx.x; k < be; k += blockDim.x) {
+          const uint64_t e = g.bent[k];
+          cmap[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+        }
+      } else {
+        table_insert(ctbl, logb, g.bent, bs, be, threadIdx.x, blockDim.x);
+      }
       {
         const uint32_t per = (d + blockDim.x - 1) / blockDim.x, j0 = threadIdx.x * per;
         uint32_t lsum = 0;
@@ -485,8 +503,16 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       };
       const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kWarpsPerCta));
       const uint32_t ce = w + 1 == kWarpsPerCta ? d : first_at((uint32_t)((uint64_t)tot * (w + 1) / kWarpsPerCta));
-      const BitmapProbe probe{ctbl, logb, (uint32_t)(g.bent[bs] >> 32), (uint32_t)(g.bent[be - 1] >> 32)};
-      const uint64_t racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe, runs[w]);
+      uint64_t racc;
+      if (direct) {
+        racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, [&](uint64_t e) -> uint32_t {
+          const uint32_t o = (uint32_t)(e >> 32) - bmin;
+          return o < span ? (uint32_t)__popc((uint32_t)e & cmap[o]) : 0u;
+        }, runs[w]);
+      } else {
+        const BitmapProbe probe{ctbl, logb, bmin, bmax};
+        racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe, runs[w]);
+      }
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
         if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[u]], (unsigned long long)s);
