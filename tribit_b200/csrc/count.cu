@@ -525,9 +525,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
     __syncthreads();
   }
   uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
-  bool cur_ok = false;
+  bool cur_ok = false, cur_direct = false;
   int logb = 0;
   uint32_t bmin = 0, bmax = 0, d = 0;
+  uint32_t* wmap = reinterpret_cast<uint32_t*>(tbl);  // the slice as a direct-mapped row
   for (;;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurVariant0 + V], kGrab);
@@ -554,12 +555,24 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
           const uint32_t bs = rp_blk(a), be = rp_blk(b), nb = be - bs;
           cur_ok = nb <= kWarpMaxBlocks;
           if (cur_ok) {
-            logb = table_logb(nb);
-            table_clear(tbl, logb, lane, 32);
-            __syncwarp();
-            table_insert(tbl, logb, g.bent, bs, be, lane, 32);
             bmin = (uint32_t)(g.bent[bs] >> 32);
             bmax = (uint32_t)(g.bent[be - 1] >> 32);
+            // A row whose blocks span at most the slice's 1,024 words is
+            // direct-mapped (one load per probe); others are hashed.
+            cur_direct = bmax - bmin < kWarpSlots * 2;
+            if (cur_direct) {
+              for (uint32_t i = lane; i <= bmax - bmin; i += 32) wmap[i] = 0u;
+              __syncwarp();
+              for (uint32_t k = bs + lane; k < be; k += 32) {
+                const uint64_t e = g.bent[k];
+                wmap[(uint32_t)(e >> 32) - bmin] = (uint32_t)e;
+              }
+            } else {
+              logb = table_logb(nb);
+              table_clear(tbl, logb, lane, 32);
+              __syncwarp();
+              table_insert(tbl, logb, g.bent, bs, be, lane, 32);
+            }
           }
         }
         __syncwarp();
@@ -573,6 +586,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       uint64_t racc;
       if (V == TRIBIT_VARIANT_MERGE) {
         racc = sweep_merge(g, tbl, d, cs, ce);
+      } else if (cur_direct) {
+        const uint32_t span = bmax - bmin + 1;
+        racc = sweep_bits(g, cs, ce, 0, 1, [&](uint64_t e) -> uint32_t {
+          const uint32_t o = (uint32_t)(e >> 32) - bmin;
+          return o < span ? (uint32_t)__popc((uint32_t)e & wmap[o]) : 0u;
+        }, runs[w]);
       } else {
         const BitmapProbe probe{tbl, logb, bmin, bmax};
         racc = sweep_bits(g, cs, ce, 0, 1, probe, runs[w]);
