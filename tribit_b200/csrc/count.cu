@@ -149,53 +149,16 @@ __device__ __forceinline__ uint64_t sweep_lists(uint32_t cs, uint32_t ce, uint32
 
 // Flattened sweep for latency-bound lists: the lists of each chunk of 32
 // slots are concatenated and lane l takes items t = base + l + 32 r, r <
-// Depth, of the concatenation; the owner slot of item t is found by a binary
-// search over the chunk's inclusive length prefix (shuffles). A lane issues
-// all Depth loads before it uses any, so a warp keeps 32 * Depth loads in
-// flight however long or short the lists are. load(k) reads item k (index
-// into the item array), probe(x) scores it; a loaded 0 must score 0.
-template <int Depth, class Desc, class Load, class Probe>
-__device__ __forceinline__ uint64_t sweep_flat(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
-                                               const Desc& desc, const Load& load, const Probe& probe) {
-  const uint32_t lane = threadIdx.x & 31;
-  uint64_t acc = 0;
-  for (uint32_t c = cs + chunk0 * 32; c < ce; c += step * 32) {
-    const uint32_t j = c + lane;
-    uint32_t ib = 0, il = 0;
-    if (j < ce) desc(j, ib, il);
-    const uint32_t incl = warp_inclusive_sum(il);
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    const uint32_t off = ib - (incl - il);  // item t of the chunk, owned by slot s, is item off_s + t
-    uint32_t racc = 0;
-    for (uint32_t base = 0; base < total; base += 32 * Depth) {
-      uint64_t x[Depth];
-#pragma unroll
-      for (int r = 0; r < Depth; ++r) {
-        const uint32_t t = base + 32 * r + lane;
-        uint32_t s = 0;
-#pragma unroll
-        for (uint32_t st = 16; st >= 1; st >>= 1) {
-          const uint32_t y = __shfl_sync(kFull, incl, s + st - 1);
-          if (y <= t) s += st;
-        }
-        const uint32_t o = __shfl_sync(kFull, off, s);
-        x[r] = t < total ? load(o + t) : 0ull;
-      }
-#pragma unroll
-      for (int r = 0; r < Depth; ++r) racc += probe(x[r]);
-    }
-    acc += racc;
-  }
-  return acc;
-}
-
-// The same flattening with the owner found incrementally: the chunk's
-// inclusive prefix and item offsets go to the warp's 64 words of shared
-// memory (wsm), each lane finds the owner of its first item once by binary
-// search and then only advances it (items of a lane only grow), so a long
-// list costs one shared-memory compare per item instead of a 5-step search.
-// Chunks whose lists average under MinAvg items keep the shuffle search
-// (measured: 8 for hub tails, 32 for bit rows).
+// Depth, of the concatenation, issuing all Depth loads before it uses any, so
+// a warp keeps 32 * Depth loads in flight however long or short the lists
+// are. load(k) reads item k (index into the item array), probe(x) scores it;
+// a loaded 0 must score 0. The owner slot of an item: the chunk's inclusive
+// prefix and item offsets go to the warp's 64 words of shared memory (wsm);
+// each lane finds the owner of its first item once by binary search and then
+// only advances it (items of a lane only grow), so a long list costs one
+// shared-memory compare per item. Chunks whose lists average under MinAvg
+// items (measured: 8 for hub tails, 32 for bit rows) find each item's owner by
+// a 5-step shuffle search over the prefix instead.
 template <int Depth, uint32_t MinAvg, class Desc, class Load, class Probe>
 __device__ __forceinline__ uint64_t sweep_runs(uint32_t cs, uint32_t ce, uint32_t chunk0, uint32_t step,
                                                const Desc& desc, const Load& load, const Probe& probe,
@@ -209,8 +172,8 @@ __device__ __forceinline__ uint64_t sweep_runs(uint32_t cs, uint32_t ce, uint32_
     const uint32_t incl = warp_inclusive_sum(il);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     if (total < 32 * MinAvg) {
-      // Short lists: a lane would cross several lists per step; the shuffle
-      // search of sweep_flat is cheaper here.
+      // Short lists: a lane would cross several lists per step; a shuffle
+      // search per item is cheaper here.
       const uint32_t offs = ib - (incl - il);
       uint32_t racc = 0;
       for (uint32_t base = 0; base < total; base += 32 * Depth) {
