@@ -1221,10 +1221,91 @@ constexpr uint32_t kHubWarpPiece = 256;         // in-edges per warp piece
 constexpr uint32_t kHubWaves = TB_HUB_WAVES;    // row ranges the hub pieces are ordered by (power of 2)
 constexpr int kHubCtasPerSm = 5;
 constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lane
+#ifndef TB_HUB_PAIRS
+#define TB_HUB_PAIRS 1
+#endif
+constexpr bool kHubPairs = TB_HUB_PAIRS != 0;   // tails read as 16-byte pairs of entries
 
 // Walks the tails of in-list entries [cs, ce) (at list) against v's staged row:
 // direct-mapped masks over blocks [bmin, bmin + span) in map, or a bucketed
 // hash (map as 8-byte slots, 2^logb buckets).
+// The hub tails' walk (see sweep_runs) with 16-byte loads: a tail's blocks are
+// read as aligned pairs of bit-row entries, so each load, address and owner
+// check serves two blocks; the pair's entries outside the tail are masked.
+// Chunks of short tails keep the per-item sweep. wsm: 128 words of the warp.
+template <int DepthPairs, class Probe>
+__device__ __forceinline__ uint64_t sweep_tail_pairs(const GraphView& g, const uint64_t* __restrict__ list,
+                                                     uint32_t cs, uint32_t ce, const Probe& probe, uint32_t* wsm) {
+  const uint32_t lane = threadIdx.x & 31;
+  const ulonglong2* __restrict__ pairs = reinterpret_cast<const ulonglong2*>(g.bent);
+  uint64_t acc = 0;
+  for (uint32_t c = cs; c < ce; c += 32) {
+    const uint32_t j = c + lane;
+    uint32_t ib = 0, il = 0;
+    if (j < ce) {
+      const uint64_t x = list[j];
+      ib = (uint32_t)(x >> 32);
+      il = (uint32_t)x;
+    }
+    const uint32_t items = warp_sum(il);
+    if (items < 32 * 8) {
+      acc += sweep_runs<2 * DepthPairs, 8>(
+          c, min(c + 32, ce), 0, 1,
+          [&](uint32_t i, uint32_t& b, uint32_t& l) {
+            const uint64_t x = list[i];
+            b = (uint32_t)(x >> 32);
+            l = (uint32_t)x;
+          },
+          [&](uint32_t k) -> uint64_t { return g.bent[k]; }, probe, wsm);
+      continue;
+    }
+    const uint32_t ie = ib + il;
+    const uint32_t p0 = ib >> 1, pn = il ? ((ie + 1) >> 1) - p0 : 0u;  // pairs covering [ib, ie)
+    const uint32_t incl = warp_inclusive_sum(pn);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    __syncwarp();
+    wsm[lane] = incl;
+    wsm[32 + lane] = p0 - (incl - pn);  // pair t of the chunk, owned by slot s, is pair off_s + t
+    wsm[64 + lane] = ib;
+    wsm[96 + lane] = ie;
+    __syncwarp();
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t st = 16; st >= 1; st >>= 1)
+      if (wsm[s + st - 1] <= lane) s += st;
+    uint32_t lim = wsm[s], off = wsm[32 + s], lo = wsm[64 + s], hi = wsm[96 + s];
+    uint32_t racc = 0;
+    for (uint32_t base = 0; base < total; base += 32 * DepthPairs) {
+      ulonglong2 x[DepthPairs];
+      uint32_t keep[DepthPairs];
+#pragma unroll
+      for (int r = 0; r < DepthPairs; ++r) {
+        const uint32_t t = base + 32 * r + lane;
+        while (t >= lim && s < 31) {
+          ++s;
+          lim = wsm[s];
+          off = wsm[32 + s];
+          lo = wsm[64 + s];
+          hi = wsm[96 + s];
+        }
+        keep[r] = 0;
+        x[r] = make_ulonglong2(0ull, 0ull);
+        if (t < total) {
+          const uint32_t p = off + t, k0 = 2 * p;
+          x[r] = pairs[p];
+          keep[r] = (k0 >= lo ? 1u : 0u) | (k0 + 1 < hi ? 2u : 0u);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < DepthPairs; ++r)
+        racc += probe((keep[r] & 1u) ? x[r].x : 0ull) + probe((keep[r] & 2u) ? x[r].y : 0ull);
+    }
+    acc += racc;
+  }
+  __syncwarp();
+  return acc;
+}
+
 __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t* __restrict__ list, uint32_t cs,
                                               uint32_t ce, bool direct, const uint32_t* map, uint32_t bmin,
                                               uint32_t bmax, int logb, uint32_t* wsm) {
@@ -1236,12 +1317,15 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   auto load = [&](uint32_t k) -> uint64_t { return g.bent[k]; };
   if (direct) {
     const uint32_t span = bmax - bmin + 1;
-    return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, [&](uint64_t e) -> uint32_t {
+    auto probe = [&](uint64_t e) -> uint32_t {
       const uint32_t o = (uint32_t)(e >> 32) - bmin;
       return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
-    }, wsm);
+    };
+    if (kHubPairs) return sweep_tail_pairs<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
+    return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
   }
   const BitmapProbe probe{reinterpret_cast<const uint64_t*>(map), logb, bmin, bmax};
+  if (kHubPairs) return sweep_tail_pairs<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
   return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
 }
 
@@ -1254,7 +1338,7 @@ __global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint6
                                                         unsigned long long* block_ns) {
   __shared__ __align__(16) uint32_t map[kHubMaxSpan];
   __shared__ uint32_t pre[kHubPiece + 1];
-  __shared__ uint32_t runs[kHubWarps][64];
+  __shared__ uint32_t runs[kHubWarps][128];
   __shared__ uint32_t s_t;
   __shared__ unsigned long long s_dt;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;

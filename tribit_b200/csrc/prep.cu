@@ -184,7 +184,7 @@ void run_edges(Arena& ar, const PrepInput& in, const uint32_t* rank, int B, cuda
   uint64_t* pos = ar.take<uint64_t>(E + 1);
   uint64_t* ptmp = take_scan_temp<uint64_t>(ar, E + 1);
   uint32_t* col = ar.take<uint32_t>(E ? E : 1);
-  uint64_t* bent = ar.take<uint64_t>(E ? E : 1);
+  uint64_t* bent = ar.take<uint64_t>(E + 2);  // + 2: 16-byte pair loads may read one entry past the end
   uint64_t* rtmp = take_scan_temp<uint64_t>(ar, n + 1);
   out->view.col = col;
   out->view.bent = bent;
