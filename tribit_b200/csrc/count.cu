@@ -1196,7 +1196,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 #define TB_HUB_PIECE 1024
 #endif
 #ifndef TB_HUB_DEPTH
-#define TB_HUB_DEPTH 8
+#define TB_HUB_DEPTH 4
 #endif
 constexpr int kHubWarps = 8;
 constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
@@ -1329,7 +1329,12 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
 }
 
-__global__ void __launch_bounds__(kHubWarps * 32) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
+// Five CTAs per SM (48 registers), the occupancy the 41 KiB of shared memory
+// allows; with four the pair loads' extra registers cost more than they save.
+#ifndef TB_HUB_MIN_CTAS
+#define TB_HUB_MIN_CTAS 5
+#endif
+__global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
                                                         const uint32_t* __restrict__ in_off,
                                                         const uint64_t* __restrict__ inl,
