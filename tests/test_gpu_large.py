@@ -1,5 +1,5 @@
-"""Larger graphs: RMAT scale 20 against the oracle, and at scale 22 the
-size-independent property that every orientation and dispatcher agrees."""
+"""Larger graphs: RMAT scales 20 and 24 against the oracle, and at scale 22
+the size-independent property that every orientation and dispatcher agrees."""
 import numpy as np
 import pytest
 
@@ -25,6 +25,22 @@ def test_planted_vs_oracle():
     with tb.Counter() as c:
         r = c.count_edges(e, n)
         assert (r.triangles, r.edges) == (want, m)
+
+
+def test_rmat24_vs_oracle():
+    """The benchmark graph itself (RMAT scale 24, edge factor 16, seed 24):
+    its count from the oracle on every host core, against the learned
+    dispatch (hash-staged hubs on every warp of the hub pass), merge and plain."""
+    import os
+    e = tb.gen_rmat(24, 16, seed=24)
+    want, m = oracle.count(e, 1 << 24, order=1, threads=max(1, os.cpu_count() or 1))
+    model = os.path.join(os.path.dirname(tb.__file__), "models", "dispatch_mlp.bin")
+    for mode in ("learned", "merge", "plain"):
+        with tb.Counter(dispatch=mode) as c:
+            if mode == "learned":
+                c.load_model(model)
+            r = c.count_edges(e, 1 << 24)
+            assert (r.triangles, r.edges) == (want, m), mode
 
 
 def test_rmat22_modes_agree():

@@ -90,6 +90,8 @@ struct BitmapProbe {
     if (blk < bmin || blk > bmax) return 0u;
     return (uint32_t)__popc((uint32_t)e & table_find(t, logb, blk));
   }
+  // e, or an entry that matches nothing.
+  static __device__ __forceinline__ uint64_t drop(uint64_t e, bool keep) { return keep ? e : 0ull; }
 };
 
 // ---- the neighbour sweep ---------------------------------------------------
@@ -1201,6 +1203,12 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 constexpr int kHubWarps = 8;
 constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
 constexpr uint32_t kHubWarpSpan = kHubMaxSpan / kHubWarps;  // spans up to this: one warp per piece
+// A warp's slice of the map: its span plus a zero word past the staged masks,
+// rounded to 16 bytes for the hash buckets (16-byte loads).
+constexpr uint32_t kHubWarpStride = kHubWarpSpan + 4;
+constexpr uint32_t kHubMapWords = kHubWarps * kHubWarpStride;  // >= kHubMaxSpan + 1
+static_assert(kHubWarpStride % 4 == 0, "warp slices hold 16-byte hash buckets");
+static_assert(kHubMapWords >= kHubMaxSpan + 1, "the CTA map needs its zero word");
 // Rows spanning more than that are staged as a bucketed hash instead (the same
 // 32 KiB, or a warp's 4 KiB slice, as 8-byte slots at most half full).
 constexpr uint32_t kHubMaxHash = kHubMaxSpan / 4;          // bit blocks: CTA hash
@@ -1298,13 +1306,36 @@ __device__ __forceinline__ uint64_t sweep_tail_pairs(const GraphView& g, const u
       }
 #pragma unroll
       for (int r = 0; r < DepthPairs; ++r)
-        racc += probe((keep[r] & 1u) ? x[r].x : 0ull) + probe((keep[r] & 2u) ? x[r].y : 0ull);
+        racc += probe(Probe::drop(x[r].x, keep[r] & 1u)) + probe(Probe::drop(x[r].y, keep[r] & 2u));
     }
     acc += racc;
   }
   __syncwarp();
   return acc;
 }
+
+#ifndef TB_HUB_CLAMP
+#define TB_HUB_CLAMP 1
+#endif
+// v's row staged as direct-mapped masks over blocks [bmin, bmin + span), with
+// map[span] = 0: a block outside the span reads that zero word instead of
+// taking a branch.
+struct DirectProbe {
+  const uint32_t* map;
+  uint32_t bmin, span;
+  __device__ __forceinline__ uint32_t operator()(uint64_t e) const {
+#if TB_HUB_CLAMP
+    return (uint32_t)__popc((uint32_t)e & map[min((uint32_t)(e >> 32) - bmin, span)]);
+#else
+    const uint32_t o = (uint32_t)(e >> 32) - bmin;
+    return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
+#endif
+  }
+  // e, or e with an empty mask: a dropped entry still probes, and matches nothing.
+  static __device__ __forceinline__ uint64_t drop(uint64_t e, bool keep) {
+    return keep ? e : (TB_HUB_CLAMP ? e & 0xFFFFFFFF00000000ull : 0ull);
+  }
+};
 
 __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t* __restrict__ list, uint32_t cs,
                                               uint32_t ce, bool direct, const uint32_t* map, uint32_t bmin,
@@ -1316,11 +1347,7 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   };
   auto load = [&](uint32_t k) -> uint64_t { return g.bent[k]; };
   if (direct) {
-    const uint32_t span = bmax - bmin + 1;
-    auto probe = [&](uint64_t e) -> uint32_t {
-      const uint32_t o = (uint32_t)(e >> 32) - bmin;
-      return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
-    };
+    const DirectProbe probe{map, bmin, bmax - bmin + 1};
     if (kHubPairs) return sweep_tail_pairs<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
     return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
   }
@@ -1341,7 +1368,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
                                                         const uint32_t* __restrict__ inrow, DeviceStats* stats,
                                                         unsigned long long* per_graph,
                                                         unsigned long long* block_ns) {
-  __shared__ __align__(16) uint32_t map[kHubMaxSpan];
+  __shared__ __align__(16) uint32_t map[kHubMapWords];
   __shared__ uint32_t pre[kHubPiece + 1];
   __shared__ uint32_t runs[kHubWarps][128];
   __shared__ uint32_t s_t;
@@ -1370,7 +1397,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     uint64_t* htbl = reinterpret_cast<uint64_t*>(map);
     const int logb = table_logb(be - bs);
     if (direct) {
-      for (uint32_t i = threadIdx.x; i < span; i += blockDim.x) map[i] = 0u;
+      for (uint32_t i = threadIdx.x; i <= span; i += blockDim.x) map[i] = 0u;  // and the zero word
     } else {
       table_clear(htbl, logb, threadIdx.x, blockDim.x);
     }
@@ -1433,7 +1460,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
   }
   // Phase 2: hubs whose row fits a warp's slice of the map, one warp per
   // piece, in wave order.
-  uint32_t* wmap = map + w * kHubWarpSpan;
+  uint32_t* wmap = map + w * kHubWarpStride;
   for (;;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurHubWarp], 1u);
@@ -1451,7 +1478,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     const bool direct = span <= kHubWarpSpan;  // else be - bs <= kHubWarpHash (schedule)
     const int logb = table_logb(be - bs);
     if (direct) {
-      for (uint32_t i = lane; i < span; i += 32) wmap[i] = 0u;
+      for (uint32_t i = lane; i <= span; i += 32) wmap[i] = 0u;  // and the zero word
       __syncwarp();
       for (uint32_t k = bs + lane; k < be; k += 32) {
         const uint64_t e = g.bent[k];
@@ -1720,13 +1747,34 @@ __global__ void k_hub_vinfo(GraphView g, uint64_t* __restrict__ vinfo) {
   vinfo[v] = x;
 }
 
-// One pass over the edges of the merge row blocks, one warp per row. For the
-// edge at CSR position j, u's tail is u's bit blocks from v's block on.
-// Mode 0: save[v] += the blocks a hub walk saves (v's row length - tail) over
-// the edges where the tail is shorter and v's span fits. Mode 1: flags those
-// edges whose hub saves at least its staging cost (span / 4 + nb stores) and
-// counts them per hub. Mode 2: appends each flagged edge's tail (first block,
-// length) and row to its hub's in-list.
+// Hub decision for the edge at CSR position j (u -> v, v's block at index pos
+// of u's bit row of nbu entries): the tail of u is shorter than v's row and v
+// can be staged; in mode 1 also v saves at least its staging cost (the direct
+// map's span / 4 vector stores, or a hash's 2 nb slots cleared, plus nb inserts).
+template <int Mode>
+__device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo,
+                                              const unsigned long long* __restrict__ save, uint32_t v,
+                                              uint32_t tail, uint32_t& nbv) {
+  const uint64_t vi = vinfo[v];
+  nbv = (uint32_t)vi;
+  const uint32_t span = (uint32_t)(vi >> 32);
+  bool hub = nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
+  if (Mode == 1)
+    hub = hub && save[v] >= (span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
+                                                 : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin);
+  return hub;
+}
+
+// One pass over the edges of the merge row blocks. Modes 0 and 1: one warp
+// per row block; rows of at most kHubLaneRow neighbours are walked by their
+// own lane, longer rows by the whole warp. Mode 2: one warp per row. For the edge at CSR position j, u's tail is u's bit
+// blocks from v's block on. Mode 0: save[v] += the blocks a hub walk saves
+// (v's row length - tail) over the candidate edges. Mode 1: flags the edges
+// whose hub saves at least its staging cost and counts them per hub. Mode 2:
+// appends each flagged edge's tail (first block, length) and row to its hub's
+// in-list. rows (may be null): the pass covers rows [rows[0], rows[1]).
+constexpr uint32_t kHubLaneRow = 64;
+
 template <int Mode>
 __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of, const uint64_t* __restrict__ vinfo,
                             unsigned long long* __restrict__ save, uint32_t* __restrict__ eflag,
@@ -1737,11 +1785,21 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
-  for (uint32_t u = u0 + warp; u < u1; u += nwarps) {
-    if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
-    const uint64_t a = g.rp[u], b = g.rp[u + 1];
-    const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a), nbu = rp_blk(b) - bs;
-    if (re - rs < 2) continue;
+  // Applies mode Mode to the edge at j (v = col[j], tail blocks) of row u.
+  auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t v, uint32_t pos, uint32_t tail, bool hub,
+                  uint32_t nbv) {
+    if (Mode == 0) {
+      if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
+    } else if (Mode == 1) {
+      if (hub) atomicAdd(&in_cnt[v], 1u);
+    } else if ((eflag[j >> 5] >> (j & 31)) & 1u) {
+      const uint32_t at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
+      inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
+      inrow[at] = u;
+    }
+  };
+  // Walks row u (CSR [rs, re), nb bit blocks from bs) with the whole warp.
+  auto warp_row = [&](uint32_t u, uint32_t rs, uint32_t re, uint32_t bs, uint32_t nb) {
     uint32_t carry = 0, prev_last = 0xFFFFFFFFu;
     for (uint32_t c = rs; c < re; c += 32) {
       const uint32_t j = c + lane;
@@ -1754,35 +1812,66 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
       const uint32_t pos = carry + incl - 1;  // index of v's block in u's bit row
       carry += __shfl_sync(kFull, incl, 31);
       prev_last = __shfl_sync(kFull, blk, 31);
-      const uint32_t tail = nbu - pos;
-      bool hub = false;
-      uint32_t nbv = 0, span = 0;
-      if (in) {
-        const uint64_t vi = vinfo[v];
-        nbv = (uint32_t)vi;
-        span = (uint32_t)(vi >> 32);
-        hub = nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
-      }
-      if (Mode == 0) {
-        if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
-      } else if (Mode == 1) {
-        // Staging cost: the direct map's span / 4 vector stores, or a hash's
-        // 2 nb slots cleared, plus nb inserts.
-        hub = hub && save[v] >= (span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
-                                                     : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin);
+      const uint32_t tail = nb - pos;
+      uint32_t nbv = 0;
+      const bool hub = in && Mode != 2 && hub_candidate<Mode>(vinfo, save, v, tail, nbv);
+      if (Mode == 1) {
         const uint32_t bits = __ballot_sync(kFull, hub);
         if (lane == 0 && bits) {
           const uint32_t sh = c & 31;
           atomicOr(&eflag[c >> 5], bits << sh);
           if (sh && (bits >> (32 - sh))) atomicOr(&eflag[(c >> 5) + 1], bits >> (32 - sh));
         }
-        if (hub) atomicAdd(&in_cnt[v], 1u);
-      } else {
-        if (in && ((eflag[j >> 5] >> (j & 31)) & 1u)) {
-          const uint32_t at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
-          inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
-          inrow[at] = u;
+      }
+      if (in) edge(u, bs, j, v, pos, tail, hub, nbv);
+    }
+  };
+  if constexpr (Mode == 2) {
+    // The in-list fill runs once per row wave over few rows: one warp per row
+    // keeps every warp of the grid busy.
+    for (uint32_t u = u0 + warp; u < u1; u += nwarps) {
+      if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
+      const uint64_t a = g.rp[u], b = g.rp[u + 1];
+      const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a);
+      if (re - rs >= 2) warp_row(u, rs, re, bs, rp_blk(b) - bs);
+    }
+  } else {
+    for (uint32_t rb = (u0 >> 5) + warp; rb < ((u1 + 31) >> 5); rb += nwarps) {
+      if (variant_of[rb] != TRIBIT_VARIANT_MERGE) continue;
+      const uint32_t u = rb * 32 + lane;
+      uint32_t rs = 0, re = 0, bs = 0, nbu = 0;
+      bool mine = u >= u0 && u < u1;
+      if (mine) {
+        const uint64_t a = g.rp[u], b = g.rp[u + 1];
+        rs = rp_row(a);
+        re = rp_row(b);
+        bs = rp_blk(a);
+        nbu = rp_blk(b) - bs;
+        mine = re - rs >= 2;
+      }
+      const bool own = mine && re - rs <= kHubLaneRow;
+      if (own) {
+        uint32_t pos = 0xFFFFFFFFu, prev = 0xFFFFFFFFu;
+        for (uint32_t j = rs; j < re; ++j) {
+          const uint32_t v = g.col[j];
+          if ((v >> 5) != prev) {
+            ++pos;
+            prev = v >> 5;
+          }
+          const uint32_t tail = nbu - pos;
+          uint32_t nbv = 0;
+          const bool hub = hub_candidate<Mode>(vinfo, save, v, tail, nbv);
+          if (Mode == 1 && hub) atomicOr(&eflag[j >> 5], 1u << (j & 31));
+          edge(u, bs, j, v, pos, tail, hub, nbv);
         }
+      }
+      // Longer rows: the warp, one row at a time.
+      uint32_t longm = __ballot_sync(kFull, mine && !own);
+      while (longm) {
+        const int r = __ffs(longm) - 1;
+        longm &= longm - 1;
+        warp_row(rb * 32 + r, __shfl_sync(kFull, rs, r), __shfl_sync(kFull, re, r), __shfl_sync(kFull, bs, r),
+                 __shfl_sync(kFull, nbu, r));
       }
     }
   }
