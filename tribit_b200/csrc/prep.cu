@@ -6,6 +6,7 @@ namespace tb {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr uint32_t kFull = 0xffffffffu;
 
 inline unsigned grid_for(uint64_t n, int per_thread = 1) {
   uint64_t g = ceil_div<uint64_t>(n, (uint64_t)kThreads * per_thread);
@@ -98,116 +99,320 @@ __global__ void k_identity_graph_of(uint64_t n, const uint64_t* voff, uint32_t G
   if (r < n) graph_of_rank[r] = graph_of_vertex(voff, G, r);
 }
 
-// Oriented key (lo << B) | hi in rank space; invalid entries and self-loops
-// become the all-ones sentinel, which sorts last and is dropped.
-template <typename K>
-__global__ void k_orient(PrepInput in, const uint32_t* __restrict__ rank, int B, K* __restrict__ keys,
-                         unsigned int* err) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const K sentinel = (K)(((unsigned __int128)1 << (2 * B)) - 1);
-  for (; i < in.E; i += stride) {
-    uint32_t a, b;
-    K key = sentinel;
-    if (load_entry(in, i, a, b, err)) {
-      uint32_t ra = rank ? rank[a] : a, rb = rank ? rank[b] : b;
-      uint32_t lo = ra < rb ? ra : rb, hi = ra < rb ? rb : ra;
-      key = ((K)lo << B) | (K)hi;
+// ---- phase 2: rows in rank space --------------------------------------------
+// Every entry is oriented from its lower-ranked endpoint lo to the higher hi.
+// A counting sort by lo (the histogram is the oriented out-degree) places the
+// hi's of each row together; each row is then sorted and deduplicated on its
+// own (rows are short: with degree order no row exceeds sqrt(2m) entries), and
+// one scan of the per-row (distinct neighbours, distinct 32-column blocks)
+// pairs gives the CSR and bit-row offsets. The 48-bit global radix sort of
+// (lo, hi) keys that this replaces took six passes over all entries.
+
+// Oriented (lo, hi) of entry i in rank space; false for dropped entries.
+__device__ __forceinline__ bool orient_entry(const PrepInput& in, const uint32_t* __restrict__ rank, uint64_t i,
+                                             uint32_t& lo, uint32_t& hi, unsigned int* err) {
+  uint32_t a, b;
+  if (!load_entry(in, i, a, b, err)) return false;
+  const uint32_t ra = rank ? rank[a] : a, rb = rank ? rank[b] : b;
+  lo = ra < rb ? ra : rb;
+  hi = ra < rb ? rb : ra;
+  return true;
+}
+
+// keys[i] = (lo << 32) | hi of entry i (kDropped for a dropped entry), and
+// cnt[lo] += 1.
+constexpr uint64_t kDropped = ~0ull;
+__global__ void k_row_count(PrepInput in, const uint32_t* __restrict__ rank, uint32_t* __restrict__ cnt,
+                            uint64_t* __restrict__ keys, unsigned int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < in.E; i += stride) {
+    uint32_t lo, hi;
+    uint64_t key = kDropped;
+    if (orient_entry(in, rank, i, lo, hi, err)) {
+      atomicAdd(&cnt[lo], 1u);
+      key = ((uint64_t)lo << 32) | hi;
     }
     keys[i] = key;
   }
 }
 
-// flags[i] = (first of a distinct key << 32) | (first of a distinct
-// (row, 32-column block)), flags[E] = 0; an exclusive scan then gives every
-// distinct edge its CSR slot and every bit-row entry its slot.
-template <typename K>
-__global__ void k_unique_flags(const K* __restrict__ keys, uint64_t E, int B, uint64_t* __restrict__ flags) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > E) return;
-  if (i == E) {
-    flags[E] = 0;
-    return;
+// nbr[cur[lo]++] = hi (cur starts as the row offsets): the only random
+// accesses are the cursors, which stay in L2.
+__global__ void k_row_fill(const uint64_t* __restrict__ keys, uint64_t E, uint32_t* __restrict__ cur,
+                           uint32_t* __restrict__ nbr) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += stride) {
+    const uint64_t key = keys[i];
+    if (key != kDropped) nbr[atomicAdd(&cur[key >> 32], 1u)] = (uint32_t)key;
   }
-  const K sentinel = (K)(((unsigned __int128)1 << (2 * B)) - 1);
-  K k = keys[i];
-  uint64_t f = 0;
-  if (k != sentinel) {
-    K p = i ? keys[i - 1] : sentinel;
-    bool is_new = (i == 0) || p != k;
-    if (is_new) {
-      const K mask = ((K)1 << B) - 1;
-      bool new_blk = (i == 0) || (p >> B) != (k >> B) || ((p & mask) >> 5) != ((k & mask) >> 5);
-      f = (1ull << 32) | (new_blk ? 1ull : 0ull);
+}
+
+constexpr uint32_t kPad = 0xFFFFFFFFu;  // sorts last; no vertex has this rank (n < 2^32)
+constexpr uint32_t kWarpSortMax = 1024;  // longer rows are sorted by a CTA
+constexpr uint32_t kCtaSortThreads = 1024;
+constexpr uint32_t kCtaSortSmem = 8192;  // longer rows are sorted in global scratch
+
+// Bitonic sort of the warp's 32 K values, value r * 32 + lane in x[r] of
+// lane lane, ascending.
+template <int K>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&x)[K]) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (uint32_t k = 2; k <= 32u * K; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const uint32_t jr = j >> 5;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+          if ((r & jr) == 0) {
+            const int p = r | (int)jr;
+            const bool up = ((r * 32u + lane) & k) == 0;
+            const uint32_t a = x[r], b = x[p];
+            const bool sw = up ? a > b : a < b;
+            x[r] = sw ? b : a;
+            x[p] = sw ? a : b;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+          const uint32_t y = __shfl_xor_sync(kFull, x[r], j);
+          const bool up = ((r * 32u + lane) & k) == 0;
+          const bool take_min = ((lane & j) == 0) == up;
+          x[r] = take_min ? min(x[r], y) : max(x[r], y);
+        }
+      }
     }
   }
-  flags[i] = f;
 }
 
-template <typename K>
-__global__ void k_unique_scatter(const K* __restrict__ keys, uint64_t E, int B, const uint64_t* __restrict__ pos,
-                                 uint32_t* __restrict__ col, uint64_t* __restrict__ bent, uint64_t* __restrict__ rp) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= E) return;
-  uint64_t p0 = pos[i], p1 = pos[i + 1];
-  uint32_t is_new = (uint32_t)((p1 >> 32) - (p0 >> 32));
-  if (!is_new) return;
-  uint32_t new_blk = (uint32_t)(p1 - p0) & 1u;  // low halves never carry
-  const K mask = ((K)1 << B) - 1;
-  K k = keys[i];
-  uint32_t row = (uint32_t)(k >> B), hi = (uint32_t)(k & mask);
-  uint32_t slot = (uint32_t)(p0 >> 32);
-  uint32_t bidx = (uint32_t)p0 + new_blk - 1u;
-  col[slot] = hi;
-  uint32_t* bw = reinterpret_cast<uint32_t*>(bent + bidx);
-  if (new_blk) bw[1] = hi >> 5;
-  atomicOr(&bw[0], 1u << (hi & 31));
-  bool row_first = (i == 0) || (uint32_t)(keys[i - 1] >> B) != row;
-  if (row_first) rp[row] = ((uint64_t)slot << 32) | bidx;
+// Sorts row a[0, L) (L <= 32 K) with the warp, writes its distinct values
+// back to a[0, u) and returns (u << 32) | distinct 32-column blocks.
+template <int K>
+__device__ __forceinline__ uint64_t warp_sort_row(uint32_t* __restrict__ a, uint32_t L) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t x[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    const uint32_t i = r * 32u + lane;
+    x[r] = i < L ? a[i] : kPad;
+  }
+  warp_bitonic<K>(x);
+  uint32_t nu = 0, nbk = 0;
+  uint32_t last = kPad;  // value 32 r - 1, from the previous register row
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    uint32_t prev = __shfl_up_sync(kFull, x[r], 1);
+    if (lane == 0) prev = last;
+    last = __shfl_sync(kFull, x[r], 31);
+    const bool first = r == 0 && lane == 0;
+    const bool is_new = x[r] != kPad && (first || x[r] != prev);
+    const bool new_blk = is_new && (first || (x[r] >> 5) != (prev >> 5));
+    const uint32_t nb = __ballot_sync(kFull, is_new);
+    if (is_new) a[nu + __popc(nb & ((1u << lane) - 1u))] = x[r];
+    nu += __popc(nb);
+    nbk += __popc(__ballot_sync(kFull, new_blk));
+  }
+  return ((uint64_t)nu << 32) | nbk;
 }
 
-__global__ void k_finalize(const uint64_t* __restrict__ pos, uint64_t E, uint64_t n, uint64_t* __restrict__ rp,
-                           DeviceStats* stats) {
-  uint64_t tot = pos[E];
-  rp[n] = tot;
+// One warp per row of at most kWarpSortMax entries (sorted in registers);
+// longer rows go to big[] for k_sort_big_rows. rows[u] = (distinct << 32) |
+// blocks, rows[n] = 0.
+__global__ void k_sort_rows(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ nbr,
+                            uint64_t* __restrict__ rows, uint32_t* __restrict__ big, uint32_t* __restrict__ nbig) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  if (warp == 0 && lane == 0) rows[n] = 0;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint32_t s = off[u], L = off[u + 1] - s;
+    uint32_t* a = nbr + s;
+    uint64_t r = 0;
+    if (L == 0) {
+    } else if (L <= 32) {
+      r = warp_sort_row<1>(a, L);
+    } else if (L <= 64) {
+      r = warp_sort_row<2>(a, L);
+    } else if (L <= 128) {
+      r = warp_sort_row<4>(a, L);
+    } else if (L <= 256) {
+      r = warp_sort_row<8>(a, L);
+    } else if (L <= 512) {
+      r = warp_sort_row<16>(a, L);
+    } else if (L <= kWarpSortMax) {
+      r = warp_sort_row<32>(a, L);
+    } else {
+      if (lane == 0) big[atomicAdd(nbig, 1u)] = u;
+      continue;
+    }
+    if (lane == 0) rows[u] = r;
+  }
+}
+
+// Rows longer than kWarpSortMax, one CTA per row: a bitonic sort of the row
+// padded to a power of two P, in shared memory (P <= kCtaSortSmem) or in the
+// row's slice [2 s, 2 s + P) of scratch (P <= 2 L), then the distinct values
+// written back to the front of the row.
+__global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_t* __restrict__ off,
+                                                                   uint32_t* __restrict__ nbr,
+                                                                   uint32_t* __restrict__ scratch,
+                                                                   uint64_t* __restrict__ rows,
+                                                                   const uint32_t* __restrict__ big,
+                                                                   const uint32_t* __restrict__ nbig) {
+  __shared__ uint32_t sm[kCtaSortSmem];
+  __shared__ uint32_t wsum[2][kCtaSortThreads / 32];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t count = *nbig;
+  for (uint32_t bi = blockIdx.x; bi < count; bi += gridDim.x) {
+    const uint32_t u = big[bi];
+    const uint32_t s = off[u], L = off[u + 1] - s;
+    uint32_t P = 1;
+    while (P < L) P <<= 1;
+    uint32_t* a = P <= kCtaSortSmem ? sm : scratch + 2ull * s;
+    for (uint32_t i = tid; i < P; i += blockDim.x) a[i] = i < L ? nbr[s + i] : kPad;
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t t = tid; t < P / 2; t += blockDim.x) {
+          const uint32_t i = 2 * j * (t / j) + (t % j);  // pairs (i, i + j)
+          const bool up = (i & k) == 0;
+          const uint32_t x = a[i], y = a[i + j];
+          if (up ? x > y : x < y) {
+            a[i] = y;
+            a[i + j] = x;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // Distinct values in order: per tile of blockDim values, a block-wide
+    // count of the new ones places them.
+    uint32_t nu = 0, nbk = 0;
+    for (uint32_t base = 0; base < L; base += blockDim.x) {
+      const uint32_t i = base + tid;
+      const uint32_t x = i < L ? a[i] : kPad;
+      const uint32_t p = i > 0 && i < L ? a[i - 1] : kPad;
+      const bool is_new = x != kPad && (i == 0 || x != p);
+      const bool new_blk = is_new && (i == 0 || (x >> 5) != (p >> 5));
+      const uint32_t bn = __ballot_sync(kFull, is_new), bb = __ballot_sync(kFull, new_blk);
+      if (lane == 0) {
+        wsum[0][w] = __popc(bn);
+        wsum[1][w] = __popc(bb);
+      }
+      __syncthreads();
+      uint32_t before = 0, tile_u = 0, tile_b = 0;
+      for (uint32_t q = 0; q < blockDim.x / 32; ++q) {
+        if (q < w) before += wsum[0][q];
+        tile_u += wsum[0][q];
+        tile_b += wsum[1][q];
+      }
+      if (is_new) nbr[s + nu + before + __popc(bn & ((1u << lane) - 1u))] = x;
+      nu += tile_u;
+      nbk += tile_b;
+      __syncthreads();  // a[] reads of this tile and wsum before the next tile
+    }
+    if (tid == 0) rows[u] = ((uint64_t)nu << 32) | nbk;
+    __syncthreads();
+  }
+}
+
+// One warp per row: the row's distinct sorted values (front of its nbr slice)
+// to col, and its bit-row entries (block << 32 | mask) to bent, each written
+// once: the mask of a block is a segmented OR over the lanes holding its
+// values (a block cut by a chunk boundary carries its partial mask over).
+__global__ void k_emit_rows(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                            const uint64_t* __restrict__ rp, uint32_t n, uint32_t* __restrict__ col,
+                            uint64_t* __restrict__ bent) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < n; u += nwarps) {
+    const uint64_t r0 = rp[u], r1 = rp[u + 1];
+    const uint32_t slot = (uint32_t)(r0 >> 32), nu = (uint32_t)(r1 >> 32) - slot, b0 = (uint32_t)r0;
+    const uint32_t* a = nbr + off[u];
+    // Blocks written so far; the previous chunk's last value and the partial
+    // mask of its last block.
+    uint32_t nblk = 0, last = kPad, carry = 0;
+    for (uint32_t c = 0; c < nu; c += 32) {
+      const uint32_t i = c + lane;
+      const bool in = i < nu;
+      const uint32_t x = in ? a[i] : kPad;
+      const uint32_t blk = x >> 5;
+      uint32_t prev = __shfl_up_sync(kFull, x, 1);
+      if (lane == 0) prev = last;
+      uint32_t next = __shfl_down_sync(kFull, x, 1);
+      if (lane == 31) next = c + 32 < nu ? a[c + 32] : kPad;
+      const bool new_blk = in && (i == 0 || blk != (prev >> 5));
+      const bool end_blk = in && (i + 1 == nu || blk != (next >> 5));
+      // Segmented OR of the block's bits from its first lane in this chunk.
+      uint32_t m = in ? 1u << (x & 31) : 0u;
+#pragma unroll
+      for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, m, o);
+        const uint32_t yb = __shfl_up_sync(kFull, blk, o);
+        if (lane >= o && yb == blk) m |= y;
+      }
+      if (i > 0 && c > 0 && blk == (last >> 5)) m |= carry;  // the block began in the previous chunk
+      const uint32_t incl = warp_inclusive_sum(new_blk ? 1u : 0u);
+      if (in) col[slot + i] = x;
+      if (end_blk) bent[b0 + nblk + incl - 1] = ((uint64_t)blk << 32) | m;
+      carry = __shfl_sync(kFull, m, 31);
+      last = __shfl_sync(kFull, x, 31);
+      nblk += __shfl_sync(kFull, incl, 31);
+    }
+  }
+}
+
+__global__ void k_finalize(const uint64_t* __restrict__ rp, uint64_t n, DeviceStats* stats) {
+  const uint64_t tot = rp[n];
   stats->edges = tot >> 32;
   stats->blocks = tot & 0xffffffffull;
 }
 
-template <typename K>
-void run_edges(Arena& ar, const PrepInput& in, const uint32_t* rank, int B, cudaStream_t st, Prepared* out,
-               DeviceStats* stats, uint64_t* rp) {
+void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t st, Prepared* out,
+              DeviceStats* stats, uint64_t* rp) {
   const uint64_t E = in.E, n = in.n;
-  K* keys = ar.take<K>(E ? E : 1);
-  K* keys_alt = ar.take<K>(E ? E : 1);
-  RadixTemp etmp = take_radix_temp(ar, E);
-  uint64_t* pos = ar.take<uint64_t>(E + 1);
-  uint64_t* ptmp = take_scan_temp<uint64_t>(ar, E + 1);
+  uint32_t* cnt = ar.take<uint32_t>(n + 1);  // row lengths, then the fill cursors
+  uint32_t* off = ar.take<uint32_t>(n + 1);
+  uint32_t* otmp = take_scan_temp<uint32_t>(ar, n + 1);
+  uint64_t* rtmp = take_scan_temp<uint64_t>(ar, n + 1);
+  uint32_t* big = ar.take<uint32_t>(n + 1);
+  uint32_t* nbig = ar.take<uint32_t>(1);
+  uint32_t* nbr = ar.take<uint32_t>(E ? E : 1);
+  uint32_t* scratch = ar.take<uint32_t>(2 * E + 2);  // the oriented keys, then long rows' sort space
   uint32_t* col = ar.take<uint32_t>(E ? E : 1);
   uint64_t* bent = ar.take<uint64_t>(E + 2);  // + 2: 16-byte pair loads may read one entry past the end
-  uint64_t* rtmp = take_scan_temp<uint64_t>(ar, n + 1);
   out->view.col = col;
   out->view.bent = bent;
   if (ar.measuring()) return;
 
-  TB_CUDA(cudaMemsetAsync(rp, 0xff, (n + 1) * sizeof(uint64_t), st));
+  const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(n, 8), 148ull * 32));
+  uint64_t* keys = reinterpret_cast<uint64_t*>(scratch);
+  TB_CUDA(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), st));
+  TB_CUDA(cudaMemsetAsync(nbig, 0, sizeof(uint32_t), st));
   if (E > 0) {
-    TB_CUDA(cudaMemsetAsync(bent, 0, E * sizeof(uint64_t), st));
-    k_orient<K><<<grid_for(E, 8), kThreads, 0, st>>>(in, rank, B, keys, &stats->err);
+    k_row_count<<<grid_for(E, 8), kThreads, 0, st>>>(in, rank, cnt, keys, &stats->err);
     TB_LAUNCH_CHECK();
-    K* sorted = radix_sort<K, NoVal, false>(keys, keys_alt, nullptr, nullptr, E, 2 * B, etmp, st, nullptr);
-    k_unique_flags<K><<<grid_for(E + 1), kThreads, 0, st>>>(sorted, E, B, pos);
-    TB_LAUNCH_CHECK();
-    device_scan<uint64_t, OpSum>(pos, pos, E + 1, true, OpSum{}, 0ull, ptmp, st);
-    k_unique_scatter<K><<<grid_for(E), kThreads, 0, st>>>(sorted, E, B, pos, col, bent, rp);
-    TB_LAUNCH_CHECK();
-  } else {
-    TB_CUDA(cudaMemsetAsync(pos, 0, sizeof(uint64_t), st));
   }
-  k_finalize<<<1, 1, 0, st>>>(pos, E, n, rp, stats);
+  device_scan<uint32_t, OpSum>(cnt, off, n + 1, true, OpSum{}, 0u, otmp, st);
+  if (E > 0) {
+    TB_CUDA(cudaMemcpyAsync(cnt, off, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    k_row_fill<<<grid_for(E, 8), kThreads, 0, st>>>(keys, E, cnt, nbr);
+    TB_LAUNCH_CHECK();
+  }
+  k_sort_rows<<<wgrid, kThreads, 0, st>>>(off, (uint32_t)n, nbr, rp, big, nbig);
   TB_LAUNCH_CHECK();
-  // Rows without edges take the start of the next row that has one.
-  device_scan<uint64_t, OpMin, true>(rp, rp, n + 1, false, OpMin{}, ~0ull, rtmp, st);
+  if (E > kWarpSortMax) {
+    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(off, nbr, scratch, rp, big, nbig);
+    TB_LAUNCH_CHECK();
+  }
+  device_scan<uint64_t, OpSum>(rp, rp, n + 1, true, OpSum{}, 0ull, rtmp, st);
+  k_emit_rows<<<wgrid, kThreads, 0, st>>>(off, nbr, rp, (uint32_t)n, col, bent);
+  TB_LAUNCH_CHECK();
+  k_finalize<<<1, 1, 0, st>>>(rp, n, stats);
+  TB_LAUNCH_CHECK();
 }
 
 }  // namespace
@@ -216,7 +421,6 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
   const uint64_t n = in.n, E = in.E;
   if (n > 0xffffffffull || E > 0xfffffffeull)
     throw StatusError(TRIBIT_ERR_TOO_LARGE, "graphs are limited to 2^32-1 vertices and 2^32-2 entries");
-  const int B = bits_for(n ? n : 1);
   DeviceStats* stats = ar.take<DeviceStats>(1);
   uint64_t* rp = ar.take<uint64_t>(n + 1);
   uint32_t* rank = nullptr;
@@ -265,11 +469,8 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
       TB_LAUNCH_CHECK();
     }
   }
-  // Phase 2: orient, sort, dedup, CSR + bit rows.
-  if (2 * B <= 32)
-    run_edges<uint32_t>(ar, in, rank, B, st, out, stats, rp);
-  else
-    run_edges<uint64_t>(ar, in, rank, B, st, out, stats, rp);
+  // Phase 2: orient, rows, sort + dedup per row, CSR + bit rows.
+  run_rows(ar, in, rank, st, out, stats, rp);
 }
 
 }  // namespace tb
