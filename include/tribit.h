@@ -89,8 +89,9 @@ typedef struct tribit_result {
   uint64_t blocks_of_threads; /* CTAs of the counting launch ("Blocks of threads") */
   uint64_t row_blocks;        /* non-empty 32-row blocks of the oriented graph */
   uint64_t row_blocks_by_variant[TRIBIT_NUM_VARIANTS];
-  float h2d_ms;               /* host -> device copy of the entries (host-input calls) */
-  float preprocess_ms;        /* fold, dedup, orient, CSR and bit-block build */
+  float h2d_ms;               /* host -> device copy of the entries (host-input calls; the degree
+                                 pass of each uploaded piece runs while the next one is copied) */
+  float preprocess_ms;        /* fold, dedup, orient, CSR and bit-block build (after the upload) */
   float kernel_ms;            /* counting kernel(s) */
   float total_ms;             /* whole call, device time */
   uint32_t count_kernels;     /* kernels one counting launch issues */

@@ -64,14 +64,22 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
   layout(c, false, in, stage, G, &L);
   cudaStream_t st = c->st;
   TB_CUDA(cudaEventRecord(c->ev[0], st));
-  if (stage && in.E) TB_CUDA(cudaMemcpyAsync(L.staged, host_entries, in.E * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
   if (G) {
     TB_CUDA(cudaMemcpyAsync(L.eoff, host_eoff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     TB_CUDA(cudaMemcpyAsync(L.voff, host_voff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     TB_CUDA(cudaMemsetAsync(L.per_graph, 0, G * sizeof(unsigned long long), st));
   }
-  TB_CUDA(cudaEventRecord(c->ev[1], st));
   tb::PrepInput pin = in;
+  if (stage && in.E) {
+    // The entries are uploaded by prepare_graph, overlapped with the degree
+    // pass; ev[1] marks the moment the last piece has landed.
+    pin.upload.host = host_entries;
+    pin.upload.copy_stream = c->copy_st;
+    pin.upload.events = c->upload_ev;
+    pin.upload.uploaded = c->ev[1];
+  } else {
+    TB_CUDA(cudaEventRecord(c->ev[1], st));
+  }
   if (stage) pin.entries = L.staged;
   if (G) {
     pin.eoff = L.eoff;
@@ -187,6 +195,8 @@ tribit_status tribit_create(const tribit_options* opts, tribit_context** out) {
     TB_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
     c->st = c->own;
     for (auto& e : c->ev) TB_CUDA(cudaEventCreate(&e));
+    TB_CUDA(cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking));
+    for (auto& e : c->upload_ev) TB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TB_CUDA(cudaMallocHost(&c->h_stats, sizeof(tb::DeviceStats)));
   });
   if (st != TRIBIT_OK) {
@@ -209,6 +219,10 @@ void tribit_destroy(tribit_context* c) {
     tb::model_free(c->model);
     for (auto& e : c->ev)
       if (e) cudaEventDestroy(e);
+    if (c->copy_st) cudaStreamSynchronize(c->copy_st);
+    for (auto& e : c->upload_ev)
+      if (e) cudaEventDestroy(e);
+    if (c->copy_st) cudaStreamDestroy(c->copy_st);
     if (c->h_stats) cudaFreeHost(c->h_stats);
     if (c->own) cudaStreamDestroy(c->own);
   }

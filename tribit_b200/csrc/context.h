@@ -25,6 +25,8 @@ struct tribit_context {
   bool prepared = false;
   tb::LaunchInfo launch{};
   cudaEvent_t ev[6] = {};
+  cudaStream_t copy_st = nullptr;                       // host uploads (overlapped with the degree pass)
+  cudaEvent_t upload_ev[tb::kUploadChunks + 1] = {};
   tb::DeviceStats* h_stats = nullptr;  // pinned
   // Tuned launch parameters (tribit_set_tuning / tribit_autotune).
   int ctas_per_sm = 0;

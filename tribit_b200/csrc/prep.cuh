@@ -43,8 +43,23 @@ struct DeviceStats {
   unsigned int overflow[8];        // overflow-list lengths
 };
 
+// Upload of host entries overlapped with the degree pass: the entries are
+// copied in kUploadChunks pieces on copy_stream, and each piece's degree pass
+// runs on the preparing stream as soon as the piece has landed. events: at
+// least kUploadChunks + 1 (the first orders the copies after the stream's
+// earlier work); uploaded is recorded on the preparing stream once every
+// piece has landed.
+constexpr int kUploadChunks = 8;
+struct HostUpload {
+  const uint64_t* host = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t* events = nullptr;
+  cudaEvent_t uploaded = nullptr;
+};
+
 struct PrepInput {
   const uint64_t* entries = nullptr;  // device, E words (a << 32) | b
+  HostUpload upload{};                // host: fill entries from upload.host first
   uint64_t E = 0;
   uint64_t n = 0;                     // vertices (sum over graphs in batch mode)
   int order = TRIBIT_ORDER_DEGREE;

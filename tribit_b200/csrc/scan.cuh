@@ -277,12 +277,13 @@ inline RadixTemp take_radix_temp(Arena& ar, uint64_t n) {
   return t;
 }
 
-// Sorts keys[0, n) on bits [0, end_bit). keys_alt (and vals_alt) are scratch of
-// the same size. Returns the buffer that holds the sorted keys (keys or
-// keys_alt); *vals_sorted receives the matching values buffer. Launches only.
+// Sorts keys[0, n) on bits [begin_bit, end_bit) (stable). keys_alt (and
+// vals_alt) are scratch of the same size. Returns the buffer that holds the
+// sorted keys (keys or keys_alt); *vals_sorted receives the matching values
+// buffer. Launches only.
 template <typename K, typename V, bool HasVals>
 K* radix_sort(K* keys, K* keys_alt, V* vals, V* vals_alt, uint64_t n, int end_bit, const RadixTemp& tmp,
-              cudaStream_t st, V** vals_sorted) {
+              cudaStream_t st, V** vals_sorted, int begin_bit = 0) {
   static_assert(sizeof(K) * kSortTile + (HasVals ? sizeof(V) * kSortTile : 0) + 4 * (kSortWarps * 256 + 512) <= 48 * 1024,
                 "radix scatter tile exceeds static shared memory");
   uint64_t tiles = ceil_div<uint64_t>(n, kSortTile);
@@ -290,7 +291,7 @@ K* radix_sort(K* keys, K* keys_alt, V* vals, V* vals_alt, uint64_t n, int end_bi
   K* dst = keys_alt;
   V* vsrc = vals;
   V* vdst = vals_alt;
-  for (int shift = 0; n > 0 && shift < end_bit; shift += 8) {
+  for (int shift = begin_bit; n > 0 && shift < end_bit; shift += 8) {
     k_radix_hist<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(src, n, shift, (uint32_t)tiles, tmp.hist);
     TB_LAUNCH_CHECK();
     device_scan<uint32_t, OpSum>(tmp.hist, tmp.hist, tiles * 256, true, OpSum{}, 0u, tmp.scan, st);
