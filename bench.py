@@ -332,6 +332,8 @@ def main():
         if mode == "learned":
             c.load_model(model_path)
         c.set_stream(stream.cuda_stream)
+        # The first call loads the kernels and sizes the arena; the second is timed.
+        c.prepare_device(d_entries.data_ptr(), d_entries.numel(), n)
         prep = c.prepare_device(d_entries.data_ptr(), d_entries.numel(), n)
         with torch.cuda.stream(stream):
             for _ in range(args.warmup):
@@ -435,7 +437,10 @@ def main():
                          "traffic_frac": traffic / (ms_per_step / 1e3) / 1e9 / peak if traffic else None},
             "cpu_baseline": cpu,
             "e2e": {"value": job_edges / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
-                    "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3},
+                    "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3,
+                    # device-timed parts of the last call (the degree pass overlaps the upload)
+                    "parts_ms": {"h2d": e2e_res.h2d_ms, "preprocess": e2e_res.preprocess_ms,
+                                 "count": e2e_res.kernel_ms}},
             "clocks": clk,
             "gpu_launches": args.steps * res.count_kernels,
         }
