@@ -1314,9 +1314,6 @@ __device__ __forceinline__ uint64_t sweep_tail_pairs(const GraphView& g, const u
   return acc;
 }
 
-#ifndef TB_HUB_CLAMP
-#define TB_HUB_CLAMP 1
-#endif
 // v's row staged as direct-mapped masks over blocks [bmin, bmin + span), with
 // map[span] = 0: a block outside the span reads that zero word instead of
 // taking a branch.
@@ -1324,16 +1321,11 @@ struct DirectProbe {
   const uint32_t* map;
   uint32_t bmin, span;
   __device__ __forceinline__ uint32_t operator()(uint64_t e) const {
-#if TB_HUB_CLAMP
     return (uint32_t)__popc((uint32_t)e & map[min((uint32_t)(e >> 32) - bmin, span)]);
-#else
-    const uint32_t o = (uint32_t)(e >> 32) - bmin;
-    return o < span ? (uint32_t)__popc((uint32_t)e & map[o]) : 0u;
-#endif
   }
   // e, or e with an empty mask: a dropped entry still probes, and matches nothing.
   static __device__ __forceinline__ uint64_t drop(uint64_t e, bool keep) {
-    return keep ? e : (TB_HUB_CLAMP ? e & 0xFFFFFFFF00000000ull : 0ull);
+    return keep ? e : e & 0xFFFFFFFF00000000ull;
   }
 };
 
