@@ -225,37 +225,91 @@ __device__ __forceinline__ uint64_t warp_sort_row(uint32_t* __restrict__ a, uint
   return ((uint64_t)nu << 32) | nbk;
 }
 
-// One warp per row of at most kWarpSortMax entries (sorted in registers);
-// longer rows go to big[] for k_sort_big_rows. rows[u] = (distinct << 32) |
-// blocks, rows[n] = 0.
-__global__ void k_sort_rows(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ nbr,
-                            uint64_t* __restrict__ rows, uint32_t* __restrict__ big, uint32_t* __restrict__ nbig) {
+// Rows of at most G entries (G = 8, 16 or 32), 32 / G at a time: lane group
+// g (lanes [g G, g G + G)) sorts the g-th row of the pass with a bitonic
+// network inside the group, then writes the row's distinct values and
+// rows[u] = (distinct << 32) | blocks. pending: the warp lanes whose rows
+// belong here; lane l's row starts at s_l with L_l entries; u = ubase + l.
+template <uint32_t G>
+__device__ __forceinline__ void sort_short_rows(uint32_t pending, uint32_t s_l, uint32_t L_l, uint32_t ubase,
+                                                uint32_t* __restrict__ nbr, uint64_t* __restrict__ rows) {
+  constexpr uint32_t R = 32 / G;
+  const uint32_t lane = threadIdx.x & 31, grp = lane / G, gl = lane % G;
+  const uint32_t gmask = G == 32 ? kFull : ((1u << G) - 1u) << (grp * G);
+  while (pending) {
+    int mine = -1;  // the warp lane whose row this group sorts in this pass
+#pragma unroll
+    for (uint32_t r = 0; r < R; ++r) {
+      const int lr = pending ? __ffs(pending) - 1 : -1;
+      if (r == grp) mine = lr;
+      pending &= pending - 1;
+    }
+    const uint32_t src = mine >= 0 ? (uint32_t)mine : 0u;
+    const uint32_t s = __shfl_sync(kFull, s_l, src), L = __shfl_sync(kFull, L_l, src);
+    uint32_t x = mine >= 0 && gl < L ? nbr[s + gl] : kPad;
+#pragma unroll
+    for (uint32_t k = 2; k <= G; k <<= 1) {
+#pragma unroll
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        const uint32_t y = __shfl_xor_sync(kFull, x, j);
+        const bool up = (gl & k) == 0;
+        x = (((lane & j) == 0) == up) ? min(x, y) : max(x, y);
+      }
+    }
+    const uint32_t prev = __shfl_up_sync(kFull, x, 1);
+    const bool first = gl == 0;
+    const bool is_new = x != kPad && (first || x != prev);
+    const bool new_blk = is_new && (first || (x >> 5) != (prev >> 5));
+    const uint32_t nb = __ballot_sync(kFull, is_new) & gmask;
+    const uint32_t nbk = __popc(__ballot_sync(kFull, new_blk) & gmask);
+    if (is_new) nbr[s + __popc(nb & ((1u << lane) - 1u))] = x;
+    if (first && mine >= 0) rows[ubase + mine] = ((uint64_t)__popc(nb) << 32) | nbk;
+  }
+}
+
+// One warp per 32-row block: rows of up to 8 and 16 entries are sorted four
+// and two at a time in lane groups, rows of up to kWarpSortMax one at a time
+// in registers; longer rows go to big[] for k_sort_big_rows. rows[u] =
+// (distinct << 32) | blocks, rows[n] = 0.
+// (Four CTAs of 256 per SM: 64 registers, no spills.)
+__global__ void __launch_bounds__(256, 4)
+    k_sort_rows(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ nbr, uint64_t* __restrict__ rows,
+                uint32_t* __restrict__ big, uint32_t* __restrict__ nbig) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   if (warp == 0 && lane == 0) rows[n] = 0;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint32_t s = off[u], L = off[u + 1] - s;
-    uint32_t* a = nbr + s;
-    uint64_t r = 0;
-    if (L == 0) {
-    } else if (L <= 32) {
-      r = warp_sort_row<1>(a, L);
-    } else if (L <= 64) {
-      r = warp_sort_row<2>(a, L);
-    } else if (L <= 128) {
-      r = warp_sort_row<4>(a, L);
-    } else if (L <= 256) {
-      r = warp_sort_row<8>(a, L);
-    } else if (L <= 512) {
-      r = warp_sort_row<16>(a, L);
-    } else if (L <= kWarpSortMax) {
-      r = warp_sort_row<32>(a, L);
-    } else {
-      if (lane == 0) big[atomicAdd(nbig, 1u)] = u;
-      continue;
+  for (uint32_t ubase = warp * 32; ubase < n; ubase += nwarps * 32) {
+    const uint32_t u = ubase + lane;
+    const bool here = u < n;
+    const uint32_t s_l = here ? off[u] : 0u, L_l = here ? off[u + 1] - s_l : 0u;
+    if (here && L_l == 0) rows[u] = 0;
+    sort_short_rows<8>(__ballot_sync(kFull, L_l >= 1 && L_l <= 8), s_l, L_l, ubase, nbr, rows);
+    sort_short_rows<16>(__ballot_sync(kFull, L_l > 8 && L_l <= 16), s_l, L_l, ubase, nbr, rows);
+    sort_short_rows<32>(__ballot_sync(kFull, L_l > 16 && L_l <= 32), s_l, L_l, ubase, nbr, rows);
+    uint32_t longer = __ballot_sync(kFull, L_l > 32);
+    while (longer) {
+      const uint32_t r = __ffs(longer) - 1;
+      longer &= longer - 1;
+      const uint32_t s = __shfl_sync(kFull, s_l, r), L = __shfl_sync(kFull, L_l, r);
+      uint32_t* a = nbr + s;
+      uint64_t res;
+      if (L <= 64) {
+        res = warp_sort_row<2>(a, L);
+      } else if (L <= 128) {
+        res = warp_sort_row<4>(a, L);
+      } else if (L <= 256) {
+        res = warp_sort_row<8>(a, L);
+      } else if (L <= 512) {
+        res = warp_sort_row<16>(a, L);
+      } else if (L <= kWarpSortMax) {
+        res = warp_sort_row<32>(a, L);
+      } else {
+        if (lane == 0) big[atomicAdd(nbig, 1u)] = ubase + r;
+        continue;
+      }
+      if (lane == 0) rows[ubase + r] = res;
     }
-    if (lane == 0) rows[u] = r;
   }
 }
 
