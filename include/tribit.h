@@ -193,7 +193,7 @@ tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, c
  * 4 x uint64) holds [0] triangles, [1] undirected edges, [2] error flags (bit 0:
  * an entry named a vertex >= num_nodes, the count is then invalid), [3] 0.
  * Returns TRIBIT_ERR_TOO_LARGE, launching nothing, for a graph whose buffers
- * do not fit the scratch array (roughly 36 bytes per entry + 40 per vertex).
+ * do not fit the scratch array (roughly 25 bytes per entry + 80 per vertex).
  * The first call on a device looks up the array's device address: make it
  * before capturing stream work on that device. All calls share the array, so
  * calls whose GPU work overlaps race: order them on one stream. */
