@@ -95,6 +95,25 @@ def test_large_parallel_path_matches(tmp_path):
 
 
 @pytest.mark.skipif(not os.path.exists("/root/reference/wiki-Vote.mtx"), reason="reference tree not mounted")
+def test_large_file_with_mixed_strict_lines_matches(tmp_path):
+    # Above the parallel threshold, lines the fast line parser leaves to the
+    # per-line strict parse (leading blanks, tabs, value columns, blank lines,
+    # self-loops) mixed with plain ones; the last line has no newline.
+    rng = np.random.default_rng(3)
+    n = 5000
+    ids = rng.integers(1, n + 1, size=(900_000, 2))
+    forms = ["{} {}", "{}\t{}", "  {} {}", "{}   {} 1.5", "{} {} -2e3", "{} {}"]
+    lines = [forms[k].format(a, b) for k, (a, b) in zip(rng.integers(0, len(forms), len(ids)), ids)]
+    lines[7] = ""
+    lines[100] = "42 42"
+    body = "%%MatrixMarket matrix coordinate real general\n% note\n" + f"{n} {n} {len(lines)}\n"
+    data = (body + "\n".join(lines)).encode()
+    assert len(data) > (8 << 20)
+    (st, nn, a), (st2, nn2, b) = both(tmp_path, data, "mixed.mtx")
+    assert st == st2 == 0 and nn == nn2 == n
+    np.testing.assert_array_equal(a, b)
+
+
 def test_wiki_vote_reader():
     st, n, a = oracle.read_mtx("/root/reference/wiki-Vote.mtx")
     n2, b = tb.read_mtx("/root/reference/wiki-Vote.mtx")

@@ -182,6 +182,40 @@ bool parse_strict(const char* p, const char* end, std::vector<uint64_t>& out) {
   return true;
 }
 
+// parse_strict into a caller array of at least (end - p) / 4 + 1 entries
+// (every entry line takes at least 4 bytes: "1 2\n"): the common line "id,
+// blanks, id, newline" is taken in one pass without a line search; any other
+// line goes through parse_strict. Returns the entries written, or SIZE_MAX
+// where parse_strict fails.
+size_t parse_strict_fast(const char* p, const char* end, uint64_t* out) {
+  size_t k = 0;
+  std::vector<uint64_t> slow;
+  while (p < end) {
+    const char* q = p;
+    uint64_t v0 = 0, v1 = 0;
+    int n0 = 0, n1 = 0;
+    while (q < end && (unsigned)(*q - '0') < 10u) v0 = v0 * 10 + (uint64_t)(*q++ - '0'), ++n0;
+    if (n0 && q < end && (*q == ' ' || *q == '\t')) {
+      while (q < end && (*q == ' ' || *q == '\t')) ++q;
+      while (q < end && (unsigned)(*q - '0') < 10u) v1 = v1 * 10 + (uint64_t)(*q++ - '0'), ++n1;
+      if (n1 && n0 <= 10 && n1 <= 10 && v0 <= 0xffffffffull && v1 <= 0xffffffffull && q < end && *q == '\n') {
+        uint64_t z;
+        if (fold((uint32_t)v0, (uint32_t)v1, &z)) out[k++] = z;
+        p = q + 1;
+        continue;
+      }
+    }
+    // Any other line: the general strict parse of this one line.
+    const char* nl = (const char*)std::memchr(p, '\n', (size_t)(end - p));
+    const char* le = nl ? nl + 1 : end;
+    slow.clear();
+    if (!parse_strict(p, le, slow)) return SIZE_MAX;
+    for (uint64_t z : slow) out[k++] = z;
+    p = le;
+  }
+  return k;
+}
+
 }  // namespace
 
 extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, uint64_t** entries,
@@ -234,6 +268,8 @@ extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, 
 
   // Entries: parallel strict parse, else the exact grammar.
   std::vector<uint64_t> all;
+  uint64_t* buf = nullptr;
+  size_t total = 0;
   const size_t body = (size_t)(end - p);
   unsigned hw = std::thread::hardware_concurrency();
   int threads = (int)std::max(1u, std::min(hw ? hw : 1u, 64u));
@@ -247,12 +283,25 @@ extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, 
     const char* x = c < end ? (const char*)std::memchr(c, '\n', (size_t)(end - c)) : nullptr;
     cut[t] = x ? x + 1 : end;
   }
-  std::vector<std::vector<uint64_t>> parts(threads);
+  std::vector<uint64_t*> parts(threads, nullptr);
+  std::vector<size_t> got(threads, 0);
   std::atomic<bool> strict_ok{true};
   auto work = [&](int t) {
-    parts[t].reserve((size_t)((cut[t + 1] - cut[t]) / 8));
-    if (!parse_strict(cut[t], cut[t + 1], parts[t])) strict_ok = false;
+    const size_t cap = (size_t)(cut[t + 1] - cut[t]) / 4 + 1;
+    parts[t] = (uint64_t*)std::malloc(cap * sizeof(uint64_t));
+    if (!parts[t]) {
+      strict_ok = false;
+      return;
+    }
+    got[t] = parse_strict_fast(cut[t], cut[t + 1], parts[t]);
+    if (got[t] == SIZE_MAX) strict_ok = false;
   };
+  struct FreeParts {
+    std::vector<uint64_t*>& v;
+    ~FreeParts() {
+      for (uint64_t* x : v) std::free(x);
+    }
+  } free_parts{parts};
   try {
     if (threads == 1) {
       work(0);
@@ -262,23 +311,36 @@ extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, 
       for (auto& x : th) x.join();
     }
     if (strict_ok) {
-      size_t total = 0;
-      for (auto& v : parts) total += v.size();
-      all.reserve(total);
-      for (auto& v : parts) all.insert(all.end(), v.begin(), v.end());
+      // Each thread copies its part into the caller's buffer.
+      std::vector<size_t> at(threads + 1, 0);
+      for (int t = 0; t < threads; ++t) at[t + 1] = at[t] + got[t];
+      total = at[threads];
+      buf = (uint64_t*)std::malloc(std::max<size_t>(total, 1) * sizeof(uint64_t));
+      if (!buf) return TRIBIT_ERR_OUT_OF_MEMORY;
+      auto copy = [&](int t) {
+        if (got[t]) std::memcpy(buf + at[t], parts[t], got[t] * sizeof(uint64_t));
+      };
+      if (threads == 1) {
+        copy(0);
+      } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < threads; ++t) th.emplace_back(copy, t);
+        for (auto& x : th) x.join();
+      }
     } else {
-      parts.clear();
       all.reserve(dims[2]);
       parse_exact(p, end, all);
+      total = all.size();
+      buf = (uint64_t*)std::malloc(std::max<size_t>(total, 1) * sizeof(uint64_t));
+      if (!buf) return TRIBIT_ERR_OUT_OF_MEMORY;
+      std::memcpy(buf, all.data(), total * sizeof(uint64_t));
     }
   } catch (const std::bad_alloc&) {
+    std::free(buf);
     return TRIBIT_ERR_OUT_OF_MEMORY;
   }
-  uint64_t* buf = (uint64_t*)std::malloc(std::max<size_t>(all.size(), 1) * sizeof(uint64_t));
-  if (!buf) return TRIBIT_ERR_OUT_OF_MEMORY;
-  std::memcpy(buf, all.data(), all.size() * sizeof(uint64_t));
   *entries = buf;
-  *n_entries = all.size();
+  *n_entries = total;
   return TRIBIT_OK;
 }
 
