@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -345,11 +346,16 @@ def read_mtx(path: str):
     ptr = _p()
     cnt = _u64()
     _check(lib.tribit_read_mtx(str(path).encode(), ctypes.byref(n), ctypes.byref(ptr), ctypes.byref(cnt)))
+    # The entries stay in the library's buffer (no copy); it is freed with the
+    # array (views keep the array, and so the buffer, alive).
+    addr = ptr.value
     try:
-        buf = (ctypes.c_uint64 * max(cnt.value, 1)).from_address(ptr.value)
-        arr = np.frombuffer(buf, dtype=np.uint64, count=cnt.value).copy()
-    finally:
-        lib.tribit_free_host(ptr)
+        buf = (ctypes.c_uint64 * max(cnt.value, 1)).from_address(addr)
+        arr = np.frombuffer(buf, dtype=np.uint64, count=cnt.value)
+        weakref.finalize(arr, lib.tribit_free_host, ctypes.c_void_p(addr))
+    except BaseException:
+        lib.tribit_free_host(ctypes.c_void_p(addr))
+        raise
     return n.value, arr
 
 
