@@ -147,6 +147,13 @@ tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning*
 /* Arithmetic of the bit-tile variant (TRIBIT_TILES_*), for later launches;
  * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_TCGEN05. */
 tribit_status tribit_set_tile_engine(tribit_context* ctx, int engine);
+/* Poll budget of the tcgen05 tile kernel's bounded mbarrier wait, for later
+ * launches (0 = the default, 2^22 polls). When one wait runs out, the CTA
+ * stops as a whole, waits (with its own bound) for the MMAs it committed,
+ * frees its TMEM and returns; tribit_read_count then reports
+ * TRIBIT_ERR_TIMEOUT. A count is therefore either exact or an error, never
+ * wrong, whatever the budget. Drops a captured launch. */
+tribit_status tribit_set_tile_wait_polls(tribit_context* ctx, uint32_t max_polls);
 /* Failure-detection test: one counting launch of the prepared graph in which
  * the tcgen05 tile kernel issues no MMA, so its bounded mbarrier wait runs out
  * after max_polls polls; the kernel frees its TMEM and returns, and
@@ -190,13 +197,20 @@ tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, c
  * (tribit_noalloc_scratch_bytes() = 32 MiB, held on each device that loads it
  * until exit). Allocates no device or host memory and needs no context.
  * Asynchronous: when the stream reaches the end of the work, d_result (device,
- * 4 x uint64) holds [0] triangles, [1] undirected edges, [2] error flags (bit 0:
- * an entry named a vertex >= num_nodes, the count is then invalid), [3] 0.
+ * 4 x uint64) holds [0] triangles, [1] undirected edges, [2] error flags
+ * (TRIBIT_NOALLOC_FLAG_*; any flag set means [0] is not a valid count), [3] 0.
  * Returns TRIBIT_ERR_TOO_LARGE, launching nothing, for a graph whose buffers
  * do not fit the scratch array (roughly 25 bytes per entry + 80 per vertex).
  * The first call on a device looks up the array's device address: make it
  * before capturing stream work on that device. All calls share the array, so
  * calls whose GPU work overlaps race: order them on one stream. */
+enum {
+  TRIBIT_NOALLOC_FLAG_ID_RANGE = 1u << 0, /* an entry named a vertex >= num_nodes */
+  TRIBIT_NOALLOC_FLAG_RESERVED = 1u << 1, /* never set */
+  TRIBIT_NOALLOC_FLAG_TIMEOUT = 1u << 2   /* a bounded wait of the tcgen05 tile kernel gave up
+                                             (the count is incomplete; tribit_count_edges
+                                             reports the same event as TRIBIT_ERR_TIMEOUT) */
+};
 tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, uint64_t n_entries, uint64_t num_nodes,
                                          uint64_t* d_result, void* stream);
 uint64_t tribit_noalloc_scratch_bytes(void);

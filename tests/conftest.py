@@ -7,7 +7,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_WIKI_VOTE = "/root/reference/wiki-Vote.mtx"
+# The reference's one shipped graph (SNAP wiki-Vote, bundled at the root of
+# sixt99/TriBIT): a copy is committed beside the other golden fixtures;
+# TRIBIT_WIKI_VOTE points the tests at another copy.
+WIKI_VOTE = os.environ.get("TRIBIT_WIKI_VOTE", os.path.join(ROOT, "tests", "golden", "wiki-Vote.mtx"))
+WIKI_VOTE_SHA256_16 = "c28b16ffed623c7f"
 
 
 def pytest_configure(config):

@@ -25,7 +25,9 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 import tribit_b200 as tb  # noqa: E402
 
-WIKI = "/root/reference/wiki-Vote.mtx"
+# The committed copy of the reference's bundled wiki-Vote.mtx (sixt99/TriBIT,
+# wiki-Vote.mtx at the repository root).
+WIKI = os.environ.get("TRIBIT_WIKI_VOTE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "wiki-Vote.mtx"))
 
 CASES = [
     # the small Chung-Lu graph: n=7,115, beta 2.0, max degree cap 1,000, ~100.8k edges
@@ -94,7 +96,7 @@ def main():
         assert st == 0
         with open(WIKI, "rb") as f:
             sha = hashlib.sha256(f.read()).hexdigest()[:16]
-        out.append(record("wiki-Vote", n, e, {"params": {"file": "wiki-Vote.mtx (reference tree)", "file_sha256_16": sha}}))
+        out.append(record("wiki-Vote", n, e, {"params": {"file": "wiki-Vote.mtx (sixt99/TriBIT root; copy in tests/golden)", "file_sha256_16": sha}}))
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_counts.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)

@@ -230,3 +230,36 @@ def test_cli_summary_block(tmp_path):
     lines = out.splitlines()
     assert lines[0].startswith("Thrust version: ") and lines[1].startswith("CUB version: ")
     assert lines[2] == f"Reading data from {p}..."
+
+
+def test_wiki_vote_reference_fixture_all_modes():
+    """The reference's one shipped graph (wiki-Vote.mtx at the root of
+    sixt99/TriBIT) under every dispatcher and both orientations: the count the
+    reference binary printed for it on a B200 (tests/golden/ref_counts.json)."""
+    from tests.conftest import WIKI_VOTE
+    ref = [r for r in json.load(open(os.path.join(ROOT, "tests", "golden", "ref_counts.json")))
+           if r["name"] == "wiki-Vote"][0]
+    assert ref["triangles"] == 608389
+    n, e = tb.read_mtx(WIKI_VOTE)
+    assert n == 8297
+    model = os.path.join(ROOT, "tribit_b200", "models", "dispatch_mlp.bin")
+    for order in ("degree", "id"):
+        for mode in MODES + ["learned"]:
+            with tb.Counter(order=order, dispatch=mode) as c:
+                if mode == "learned":
+                    c.load_model(model)
+                r = c.count_edges(e, n)
+                assert (r.triangles, r.edges) == (ref["triangles"], 100762), (order, mode)
+                assert c.count_mtx(WIKI_VOTE).triangles == ref["triangles"], (order, mode)
+
+
+def test_cli_on_wiki_vote_matches_reference_binary():
+    from tests.conftest import WIKI_VOTE
+    ref = [r for r in json.load(open(os.path.join(ROOT, "tests", "golden", "ref_counts.json")))
+           if r["name"] == "wiki-Vote"][0]
+    cli = os.path.join(ROOT, "tribit_b200", "bin", "tribit")
+    r = subprocess.run([cli, "-i", WIKI_VOTE], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    # the reference harness regexes (artifact/sc26/run_benchmarks/run_single_gpu.py:78-83)
+    assert int(re.search(r"Triangles\s*:\s*(\d+)", r.stdout).group(1)) == ref["triangles"]
+    assert f"Graph              : {WIKI_VOTE}" in r.stdout

@@ -86,3 +86,25 @@ def test_tile_wait_times_out_and_the_context_recovers():
         c.prepare_device(d.data_ptr(), d.numel(), n)
         c.launch_count()
         assert c.read_count().triangles == 8 * comb(256)
+
+
+@pytest.mark.parametrize("polls", [1, 2, 3, 4, 8, 16, 64, 256, 4096])
+def test_tile_wait_budget_gives_exact_count_or_timeout(polls):
+    # With a poll budget near the MMA's own latency some CTAs' waits succeed
+    # and some run out. The decision is taken for the whole CTA, the committed
+    # MMAs are drained before TMEM is freed, and the launch reports either the
+    # exact count or TRIBIT_ERR_TIMEOUT -- never a wrong count.
+    n, e = cliques_on_consecutive_ids([256] * 24)
+    want = 24 * comb(256)
+    with tb.Counter(dispatch="mma") as c:
+        c.set_tile_engine("tcgen05")
+        c.set_tile_wait_polls(polls)
+        for _ in range(3):
+            try:
+                r = c.count_edges(e, n)
+            except tb.TribitError as ex:
+                assert ex.status == 10  # TRIBIT_ERR_TIMEOUT
+                continue
+            assert r.triangles == want and r.row_blocks_by_variant[0] > 0
+        c.set_tile_wait_polls(0)  # the default budget
+        assert c.count_edges(e, n).triangles == want

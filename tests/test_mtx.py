@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
+from tests.conftest import WIKI_VOTE
 import tribit_b200 as tb
 
 HDR = "%%MatrixMarket matrix coordinate pattern general\n"
@@ -94,7 +95,6 @@ def test_large_parallel_path_matches(tmp_path):
     assert len(a) == len(e) - 1 - int(np.sum((e >> np.uint64(32)) == (e & np.uint64(0xFFFFFFFF)))) or len(a) < len(e)
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/wiki-Vote.mtx"), reason="reference tree not mounted")
 def test_large_file_with_mixed_strict_lines_matches(tmp_path):
     # Above the parallel threshold, lines the fast line parser leaves to the
     # per-line strict parse (leading blanks, tabs, value columns, blank lines,
@@ -115,8 +115,8 @@ def test_large_file_with_mixed_strict_lines_matches(tmp_path):
 
 
 def test_wiki_vote_reader():
-    st, n, a = oracle.read_mtx("/root/reference/wiki-Vote.mtx")
-    n2, b = tb.read_mtx("/root/reference/wiki-Vote.mtx")
+    st, n, a = oracle.read_mtx(WIKI_VOTE)
+    n2, b = tb.read_mtx(WIKI_VOTE)
     assert st == 0 and n == n2 == 8297
     np.testing.assert_array_equal(a, b)
 

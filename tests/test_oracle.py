@@ -1,4 +1,5 @@
 """The CPU oracle against closed-form known answers and the golden fixtures."""
+import hashlib
 import json
 import os
 
@@ -6,6 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
+from tests.conftest import WIKI_VOTE, WIKI_VOTE_SHA256_16
 import tribit_b200 as tb
 from tests.graphs import clique, comb, numpy_count, star, wheel, zip_pairs
 
@@ -70,10 +72,11 @@ def test_golden_generated(case):
     assert oracle.count_tribit(e, n) == (case["triangles"], case["reference_blocks_of_threads"])
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/wiki-Vote.mtx"), reason="reference tree not mounted")
 def test_wiki_vote_reference_fixture():
     rec = [c for c in GOLDEN if c["name"] == "wiki-Vote"][0]
-    st, n, e = oracle.read_mtx("/root/reference/wiki-Vote.mtx")
+    with open(WIKI_VOTE, "rb") as f:
+        assert hashlib.sha256(f.read()).hexdigest()[:16] == rec["params"]["file_sha256_16"] == WIKI_VOTE_SHA256_16
+    st, n, e = oracle.read_mtx(WIKI_VOTE)
     assert st == 0 and n == rec["num_nodes"] == 8297 and len(e) == rec["entries"]
     assert oracle.count(e, n) == (608389, 100762)
     assert oracle.count_tribit(e, n) == (608389, 28449)

@@ -15,6 +15,7 @@ run every other test; it also passes on its own in a fresh process.
 import numpy as np
 import pytest
 
+import oracle
 import tribit_b200 as tb
 
 pytestmark = pytest.mark.gpu
@@ -34,6 +35,8 @@ def test_noalloc_matches_counted_entry_point_twice():
     graphs = _graphs()
     with tb.Counter() as c:
         want = [c.count_edges(e, n) for n, e in graphs]
+    # The context entry point is itself pinned to the oracle; check it here too.
+    assert [(w.triangles, w.edges) for w in want] == [oracle.count(e, n) for n, e in graphs]
     stream = torch.cuda.Stream()
     out = torch.empty(4, dtype=torch.int64, device="cuda")
     for call in range(2):

@@ -107,6 +107,7 @@ _decl("tribit_set_tuning", ctypes.c_int, _p, ctypes.POINTER(Tuning))
 _decl("tribit_autotune", ctypes.c_int, _p, _u32, ctypes.POINTER(Tuning))
 _decl("tribit_set_tile_engine", ctypes.c_int, _p, ctypes.c_int)
 _decl("tribit_test_tile_timeout", ctypes.c_int, _p, _u32)
+_decl("tribit_set_tile_wait_polls", ctypes.c_int, _p, _u32)
 _decl("tribit_capture_count", ctypes.c_int, _p)
 _decl("tribit_read_batch_counts", ctypes.c_int, _p, _p, _u32)
 _decl("tribit_gen_batch", ctypes.c_int, _u32, _u32, _u32, _u64, _p, _p, _p)
@@ -212,6 +213,11 @@ class Counter:
     def set_tile_engine(self, engine: str):
         """Arithmetic of the bit-tile variant: "mma_sync" (b1 AND+POPC) or "tcgen05" (kind::i8)."""
         _check(lib.tribit_set_tile_engine(self._h, TILE_ENGINES.index(engine)), self._h)
+
+    def set_tile_wait_polls(self, max_polls: int):
+        """Poll budget of the tcgen05 tiles' bounded wait (0 = default); a
+        launch whose wait runs out reports TRIBIT_ERR_TIMEOUT, never a wrong count."""
+        _check(lib.tribit_set_tile_wait_polls(self._h, max_polls), self._h)
 
     def autotune(self, reps: int = 2) -> Tuning:
         t = Tuning()

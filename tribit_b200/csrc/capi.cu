@@ -94,9 +94,7 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
   c->prepared = true;
   TB_CUDA(cudaEventRecord(c->ev[2], st));
   if (count) {
-    tb::CountConfig cfg;
-    cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->ctas_per_sm;
+    tb::CountConfig cfg = tb::count_config(c);
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, L.per_graph, cfg, st);
   }
   TB_CUDA(cudaEventRecord(c->ev[3], st));
@@ -106,7 +104,7 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
   TB_CUDA(cudaGetLastError());
   const tb::DeviceStats& hs = *c->h_stats;
   if (hs.err & tb::kErrIdRange) throw StatusError(TRIBIT_ERR_ID_RANGE, "an entry names a vertex id >= num_nodes");
-  if (hs.err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
+  if (hs.count_err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
   if (res) {
     std::memset(res, 0, sizeof *res);
     res->triangles = count ? hs.triangles : 0;
@@ -292,9 +290,7 @@ tribit_status tribit_launch_count(tribit_context* c) {
       TB_CUDA(cudaGraphLaunch(c->graph_exec, c->st));
       return;
     }
-    tb::CountConfig cfg;
-    cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->ctas_per_sm;
+    tb::CountConfig cfg = tb::count_config(c);
     if (c->num_graphs) TB_CUDA(cudaMemsetAsync(c->per_graph, 0, c->num_graphs * sizeof(unsigned long long), c->st));
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
   });
@@ -305,9 +301,7 @@ tribit_status tribit_capture_count(tribit_context* c) {
   return guarded(c, [&] {
     DeviceGuard dg(c->device);
     tb::drop_graph(c);
-    tb::CountConfig cfg;
-    cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->ctas_per_sm;
+    tb::CountConfig cfg = tb::count_config(c);
     // One ordinary launch first: one-time function attributes are set outside the capture.
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
     TB_CUDA(cudaStreamSynchronize(c->st));
@@ -368,14 +362,20 @@ tribit_status tribit_set_tile_engine(tribit_context* c, int engine) {
   });
 }
 
+tribit_status tribit_set_tile_wait_polls(tribit_context* c, uint32_t max_polls) {
+  if (!c) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->tile_wait_polls = max_polls;
+    tb::drop_graph(c);
+  });
+}
+
 tribit_status tribit_test_tile_timeout(tribit_context* c, uint32_t max_polls) {
   if (!c || !c->prepared || max_polls == 0) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     DeviceGuard dg(c->device);
     tb::drop_graph(c);
-    tb::CountConfig cfg;
-    cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->ctas_per_sm;
+    tb::CountConfig cfg = tb::count_config(c);
     cfg.tile_wait_polls = max_polls;
     cfg.tile_test_no_commit = 1;
     c->launch = tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);
@@ -400,9 +400,7 @@ tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* b
         if (st != TRIBIT_OK) return st;
         st = guarded(c, [&] {
           DeviceGuard dg(c->device);
-          tb::CountConfig cfg;
-          cfg.num_sms = c->num_sms;
-          cfg.ctas_per_sm = c->ctas_per_sm;
+          tb::CountConfig cfg = tb::count_config(c);
           tb::launch_count(c->prep.view, c->sched, c->prep.stats, c->per_graph, cfg, c->st);  // warm
           std::vector<float> ms(reps);
           for (uint32_t r = 0; r < reps; ++r) {
@@ -430,7 +428,7 @@ tribit_status tribit_read_count(tribit_context* c, tribit_result* out) {
     TB_CUDA(cudaMemcpyAsync(c->h_stats, c->prep.stats, sizeof(tb::DeviceStats), cudaMemcpyDeviceToHost, c->st));
     TB_CUDA(cudaStreamSynchronize(c->st));
     TB_CUDA(cudaGetLastError());
-    if (c->h_stats->err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
+    if (c->h_stats->count_err & tb::kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
     if (out) {
       std::memset(out, 0, sizeof *out);
       out->triangles = c->h_stats->triangles;

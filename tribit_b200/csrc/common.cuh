@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -66,10 +67,26 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// Runs fn() once per CUDA device (the current one when called), for settings
+// such as cudaFuncSetAttribute that apply per device. Thread-safe; a call whose
+// fn throws leaves the device unmarked, so a later call retries it.
+template <int Tag, typename F>
+void once_per_device(F&& fn) {
+  constexpr int kMaxDevices = 64;
+  static std::once_flag flags[kMaxDevices];
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice", __FILE__, __LINE__);
+  if (dev < 0 || dev >= kMaxDevices) {
+    fn();
+    return;
+  }
+  std::call_once(flags[dev], fn);
+}
+
 // Device-side error flags shared by the preprocessing and counting kernels.
 enum : uint32_t {
   kErrIdRange = 1u << 0,    // an entry named a vertex >= num_nodes
-  kErrTableFull = 1u << 1,  // a row did not fit the lookup table it was routed to
+  kErrReserved = 1u << 1,   // never set (kept so the flag values stay those of the C-ABI)
   kErrTimeout = 1u << 2,    // a bounded wait gave up
 };
 

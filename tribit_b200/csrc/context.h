@@ -33,6 +33,7 @@ struct tribit_context {
   uint32_t piece_width = 64;
   int tile_engine = TRIBIT_TILES_TCGEN05;  // measured faster than mma.sync on dense tiles
   float tile_min_nnz = 64.f;
+  uint32_t tile_wait_polls = 0;        // tcgen05 tiles' bounded mbarrier wait (0: the default budget)
   uint32_t num_graphs = 0;             // batch size of the prepared input (0: single graph)
   cudaGraph_t graph = nullptr;         // captured counting launch (tribit_capture_count)
   cudaGraphExec_t graph_exec = nullptr;
@@ -80,6 +81,15 @@ tribit_status guarded(tribit_context* ctx, F&& body) {
 // Rebuilds the context's schedule for its dispatch mode (learned mode runs the
 // MLP over full features) with its tuned piece width and tile threshold.
 void apply_dispatch(tribit_context* c, cudaStream_t st);
+
+// Launch configuration of the context's counting kernels.
+inline CountConfig count_config(const tribit_context* c) {
+  CountConfig cfg;
+  cfg.num_sms = c->num_sms;
+  cfg.ctas_per_sm = c->ctas_per_sm;
+  if (c->tile_wait_polls) cfg.tile_wait_polls = c->tile_wait_polls;
+  return cfg;
+}
 
 // Drops a captured counting graph (the schedule it was captured from changed).
 inline void drop_graph(tribit_context* c) {

@@ -10,6 +10,8 @@
 // flattened across lanes. Rows whose structure does not fit a warp's slice go
 // whole to a CTA-wide pass, and rows too large for that to a global-memory
 // pass, so every piece of every list is counted exactly once.
+#include <cstddef>
+
 #include "count.cuh"
 #include "scan.cuh"
 
@@ -814,6 +816,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
 
 constexpr int kTcThreads = 128;
 constexpr uint32_t kTcChunk = 256;                 // K bytes (columns) unpacked per round
+constexpr uint32_t kTcDrainPolls = 1u << 22;       // bounded wait for committed MMAs after a failed wait
 
 
 struct TcSmem {
@@ -1031,11 +1034,14 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
                            smem_addr(&sm.mbar))
                        : "memory");
         }
-        const bool ok = tc_wait(&sm.mbar, phase, max_polls);
+        // One decision for the whole CTA: a thread whose own polls ran out
+        // fails the chunk for every thread, so all threads leave the loop
+        // together and no TMEM load follows a failed wait.
+        const bool ok = __syncthreads_and(tc_wait(&sm.mbar, phase, max_polls) ? 1 : 0) != 0;
         phase ^= 1u;
         if (!ok) {
           if (tid == 0) {
-            atomicOr(&stats->err, kErrTimeout);
+            atomicOr(&stats->count_err, kErrTimeout);
             sm.fail = 1;
           }
           break;
@@ -1072,9 +1078,11 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
     if (block_ns && tid == 0) atomicAdd(&block_ns[rb], (cycles() - t_start) * (kTcThreads / 32));
   }
   __syncthreads();
-  // After a failed wait, give the outstanding MMAs one more bounded wait
-  // before their accumulator columns are freed.
-  if (sm.fail) tc_wait(&sm.mbar, phase ^ 1u, max_polls);
+  // After a failed wait, the MMAs of the failed chunk may still be running
+  // (they were committed; only the wait gave up): give them one more bounded
+  // wait of their own budget before their accumulator columns are freed. With
+  // nothing committed (the failure-detection test) there is nothing to drain.
+  if (sm.fail && !test_no_commit) tc_wait(&sm.mbar, phase ^ 1u, kTcDrainPolls);
   __syncthreads();
   if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
   acc = warp_sum(acc);
@@ -2112,20 +2120,22 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
                         const CountConfig& cfg, cudaStream_t st) {
   GraphView g = graph;
   g.eflag = s.hubs_active ? s.eflag : nullptr;
-  static bool attr_done = false;
-  if (!attr_done) {
+  once_per_device<0>([] {
     TB_CUDA(cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(uint64_t) << kCtaLogSlots)));
     TB_CUDA(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kTileWarps * sizeof(TileSmem))));
     TB_CUDA(cudaFuncSetAttribute(k_tiles_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
-    attr_done = true;
-  }
+  });
   const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
   const int per_sm = cfg.ctas_per_sm > 0 ? cfg.ctas_per_sm : 6;
   const unsigned warp_grid = (unsigned)(sms * per_sm);
   LaunchInfo info;
-  TB_CUDA(cudaMemsetAsync(stats->cursor, 0, sizeof(stats->cursor) + sizeof(stats->overflow), st));
+  static_assert(offsetof(DeviceStats, cursor) == offsetof(DeviceStats, count_err) + sizeof(unsigned int) &&
+                    offsetof(DeviceStats, overflow) == offsetof(DeviceStats, cursor) + sizeof(DeviceStats::cursor),
+                "count_err, cursor and overflow are cleared by one memset");
+  TB_CUDA(cudaMemsetAsync(&stats->count_err, 0,
+                          sizeof(stats->count_err) + sizeof(stats->cursor) + sizeof(stats->overflow), st));
   TB_CUDA(cudaMemsetAsync(&stats->triangles, 0, sizeof(stats->triangles), st));
   uint32_t* ovf_cta = s.overflow;
   uint32_t* ovf_global = s.overflow + s.overflow_cap;

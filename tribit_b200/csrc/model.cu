@@ -252,12 +252,11 @@ __global__ void __launch_bounds__(kModelThreads) k_dispatch(const float* __restr
 constexpr size_t kModelSmem = sizeof(SmemModel);
 
 void set_smem_attrs() {
-  static bool done = false;
-  if (done) return;
-  TB_CUDA(cudaFuncSetAttribute(k_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
-  TB_CUDA(cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
-  TB_CUDA(cudaFuncSetAttribute(k_dispatch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
-  done = true;
+  once_per_device<1>([] {
+    TB_CUDA(cudaFuncSetAttribute(k_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
+    TB_CUDA(cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
+    TB_CUDA(cudaFuncSetAttribute(k_dispatch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kModelSmem));
+  });
 }
 
 unsigned grid_warps(uint64_t rows) {
@@ -520,9 +519,7 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     if (nrb) TB_CUDA(cudaMemsetAsync(c->sched.variant_of, variant, nrb, c->st));
     c->sched.hubs = variant == TRIBIT_VARIANT_MERGE;
     tb::build_pieces(c->prep.view, c->sched, c->st);
-    tb::CountConfig cfg;
-    cfg.num_sms = c->num_sms;
-    cfg.ctas_per_sm = c->ctas_per_sm;
+    tb::CountConfig cfg = tb::count_config(c);
     cfg.block_ns = ns;
     cfg.variant_start = c->ev[0];
     cfg.variant_stop = c->ev[1];

@@ -44,10 +44,14 @@ std::mutex g_setup_mu;
 void* g_scratch_addr[kMaxDevices] = {};
 int g_num_sms[kMaxDevices] = {};
 
+static_assert((uint32_t)tb::kErrIdRange == (uint32_t)TRIBIT_NOALLOC_FLAG_ID_RANGE &&
+                  (uint32_t)tb::kErrTimeout == (uint32_t)TRIBIT_NOALLOC_FLAG_TIMEOUT,
+              "d_result[2] carries the device flags as the header documents them");
+
 __global__ void k_noalloc_result(const tb::DeviceStats* stats, unsigned long long* out) {
   out[0] = stats->triangles;
   out[1] = stats->edges;
-  out[2] = stats->err;
+  out[2] = stats->err | stats->count_err;
   out[3] = 0ull;
 }
 

@@ -37,8 +37,8 @@ struct DeviceStats {
   unsigned long long triangles;
   unsigned long long edges;        // undirected edges after dedup (m)
   unsigned long long blocks;       // bit-row entries (nb)
-  unsigned int err;                // kErr* flags
-  unsigned int pad;
+  unsigned int err;                // kErr* flags of the preprocessing
+  unsigned int count_err;          // kErr* flags of the latest counting launch (cleared by each launch)
   unsigned int cursor[8];          // work cursors of the counting kernels
   unsigned int overflow[8];        // overflow-list lengths
 };
