@@ -136,6 +136,9 @@ typedef struct tribit_tuning {
   float tile_min_nnz;   /* plain dispatch: fewest edges of a row block sent to the bit tiles, which
                            also need 1/8 of the tile's cells set (default 64; 1e30 = off) */
   float count_ms;       /* tribit_autotune: measured counting time of this setting */
+  float merge_ratio;    /* plain dispatch: a row block not sent to the tiles goes to the sorted-list
+                           merge when its neighbours' bit rows average at least merge_ratio times
+                           its own rows' length, else to the bitmap sweep (default 2; 1e30 = never) */
 } tribit_tuning;
 tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);
 /* Applies to later calls, and rebuilds the schedule of the prepared graph. */
@@ -244,6 +247,10 @@ tribit_status tribit_model_train(tribit_context* ctx, const float* x, const floa
 /* Features of every 32-row block (num_row_blocks x 16 floats; out may be NULL
  * to query the count). */
 tribit_status tribit_block_features(tribit_context* ctx, float* out, uint64_t cap, uint64_t* num_row_blocks);
+/* The counting variant (TRIBIT_VARIANT_*) the context's dispatcher chose for
+ * every 32-row block (out may be NULL to query the count). Blocks without
+ * work keep their choice but get no pieces. */
+tribit_status tribit_block_variants(tribit_context* ctx, uint8_t* out, uint64_t cap, uint64_t* num_row_blocks);
 /* Counts with every row block on `variant` (TRIBIT_VARIANT_*) and records the
  * SM cycles each row block's pieces took (cycles_out[num_row_blocks]);
  * *triangles receives the count, which equals the normal one, and

@@ -49,6 +49,9 @@ _decl("oracle_count_csr_sample", _u64, ctypes.POINTER(_CSR), ctypes.c_int, _u64,
 _decl("oracle_count_rows", None, ctypes.POINTER(_CSR), _p)
 _decl("oracle_count_entries", _u64, _p, _u64, _u64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_u64))
 _decl("oracle_count_tribit", _u64, _p, _u64, _u64, ctypes.POINTER(_u64))
+_decl("oracle_write_mtx", ctypes.c_int, ctypes.c_char_p, _u64, _p, _u64)
+_decl("oracle_gen_rmat", ctypes.c_int, ctypes.c_int, _u64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _u64,
+      ctypes.c_int, _p)
 
 
 def _arr(a):
@@ -126,3 +129,23 @@ class CSR:
             self._g = None
 
     __del__ = close
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1,
+             threads: int | None = None) -> np.ndarray:
+    """Seeded R-MAT entries, identical to tribit_b200.gen_rmat, without the product library."""
+    if threads is None:
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    out = np.empty(edge_factor << scale, dtype=np.uint64)
+    st = _lib.oracle_gen_rmat(scale, edge_factor, a, b, c, seed, threads, out.ctypes.data)
+    if st != 0:
+        raise ValueError(f"oracle_gen_rmat failed with status {st}")
+    return out
+
+
+def write_mtx(path, num_nodes: int, entries):
+    """Entries -> symmetric pattern .mtx (the reference binary's input format)."""
+    e = _arr(entries)
+    st = _lib.oracle_write_mtx(str(path).encode(), num_nodes, e.ctypes.data, e.size)
+    if st != 0:
+        raise OSError(f"oracle_write_mtx({path}) failed with status {st}")

@@ -5,6 +5,7 @@
 #include "oracle.h"
 
 #include <ctype.h>
+#include <math.h>
 #include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -502,4 +503,118 @@ uint64_t oracle_count_tribit(const uint64_t* entries, uint64_t n_entries, uint64
   free(ucol);
   free(lcol);
   return tri;
+}
+
+/* ---- seeded R-MAT generator (for the reference arm of the benchmark) ------
+ * The benchmark's reference arm must not load the product library, yet it has
+ * to count the same graph. This restates the product's counter-based R-MAT
+ * generator (Chakrabarti, Zhan and Faloutsos, SDM 2004) from its definition:
+ * entry i draws one SplitMix64 value per two levels, stream value
+ * mix(mix(seed) ^ (i * 32 + level / 2) * 0xD6E8FEB86659FD93), and at level l
+ * the (l & 1)-th 32-bit half picks a quadrant against the cumulative 32-bit
+ * thresholds floor(p * 2^32) of a, a + b, a + b + c: b sets the column bit,
+ * c the row bit, d both. Word i = (row << 32) | col. A CPU test checks it
+ * against the product's tribit_gen_rmat word for word. */
+static uint64_t g_splitmix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static uint32_t g_threshold(double p) {
+  double t = floor(p * 4294967296.0);
+  if (t < 0) t = 0;
+  if (t > 4294967295.0) t = 4294967295.0;
+  return (uint32_t)t;
+}
+
+typedef struct {
+  uint64_t seed_mix, lo, hi;
+  int scale;
+  uint32_t ta, tab, tabc;
+  uint64_t* out;
+} rmat_job;
+
+static void* rmat_worker(void* arg) {
+  const rmat_job* j = (const rmat_job*)arg;
+  for (uint64_t i = j->lo; i < j->hi; ++i) {
+    uint32_t r = 0, c = 0;
+    uint64_t h = 0;
+    for (int l = 0; l < j->scale; ++l) {
+      if ((l & 1) == 0) h = g_splitmix(j->seed_mix ^ (((i << 5) | (uint64_t)(l >> 1)) * 0xD6E8FEB86659FD93ull));
+      const uint32_t x = (uint32_t)(h >> ((l & 1) * 32));
+      const uint32_t bit = 1u << (j->scale - 1 - l);
+      if (x >= j->tabc) {
+        r |= bit;
+        c |= bit;
+      } else if (x >= j->tab) {
+        r |= bit;
+      } else if (x >= j->ta) {
+        c |= bit;
+      }
+    }
+    j->out[i] = ((uint64_t)r << 32) | c;
+  }
+  return NULL;
+}
+
+int oracle_gen_rmat(int scale, uint64_t edge_factor, double a, double b, double c, uint64_t seed, int threads,
+                    uint64_t* out) {
+  if (scale < 1 || scale > 31 || !out || a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return 1;
+  if (threads < 1) threads = 1;
+  const uint64_t m = edge_factor << scale;
+  rmat_job* jobs = (rmat_job*)malloc(sizeof(rmat_job) * (size_t)threads);
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)threads);
+  if (!jobs || !th) {
+    free(jobs);
+    free(th);
+    return 8;
+  }
+  const uint64_t chunk = (m + (uint64_t)threads - 1) / (uint64_t)threads;
+  for (int k = 0; k < threads; ++k) {
+    jobs[k].seed_mix = g_splitmix(seed);
+    jobs[k].lo = (uint64_t)k * chunk < m ? (uint64_t)k * chunk : m;
+    jobs[k].hi = jobs[k].lo + chunk < m ? jobs[k].lo + chunk : m;
+    jobs[k].scale = scale;
+    jobs[k].ta = g_threshold(a);
+    jobs[k].tab = g_threshold(a + b);
+    jobs[k].tabc = g_threshold(a + b + c);
+    jobs[k].out = out;
+    pthread_create(&th[k], NULL, rmat_worker, &jobs[k]);
+  }
+  for (int k = 0; k < threads; ++k) pthread_join(th[k], NULL);
+  free(jobs);
+  free(th);
+  return 0;
+}
+
+/* Writes entries as a symmetric pattern Matrix Market file, one 1-based
+ * "max min" line per entry (self-loops and duplicates kept as given), the
+ * input the reference's read_mtx (tribit.cu:228-269) parses. 0 ok, 2 I/O. */
+int oracle_write_mtx(const char* path, uint64_t num_nodes, const uint64_t* entries, uint64_t n_entries) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return 2;
+  char* buf = (char*)malloc(1 << 22);
+  if (!buf) {
+    fclose(f);
+    return 8;
+  }
+  size_t used = (size_t)snprintf(buf, 256, "%%%%MatrixMarket matrix coordinate pattern symmetric\n%llu %llu %llu\n",
+                                 (unsigned long long)num_nodes, (unsigned long long)num_nodes,
+                                 (unsigned long long)n_entries);
+  int bad = 0;
+  for (uint64_t i = 0; i < n_entries && !bad; ++i) {
+    const uint32_t a = (uint32_t)(entries[i] >> 32), b = (uint32_t)entries[i];
+    const uint32_t hi = a > b ? a : b, lo = a > b ? b : a;
+    used += (size_t)snprintf(buf + used, 32, "%u %u\n", hi + 1, lo + 1);
+    if (used > (1 << 22) - 64) {
+      bad = fwrite(buf, 1, used, f) != used;
+      used = 0;
+    }
+  }
+  if (!bad && used) bad = fwrite(buf, 1, used, f) != used;
+  free(buf);
+  if (fclose(f) != 0) bad = 1;
+  return bad ? 2 : 0;
 }

@@ -76,6 +76,16 @@ uint64_t oracle_count_tribit(const uint64_t* entries, uint64_t n_entries, uint64
  * folded, deduplicated, sorted edges; cheap at any size. */
 uint64_t oracle_tribit_blocks(const uint64_t* edges, uint64_t m);
 
+/* Seeded R-MAT entries, word for word those of the product's tribit_gen_rmat
+ * (edge_factor << scale words, (row << 32) | col, duplicates and self-loops
+ * kept), on `threads` host threads. 0 ok, 1 bad argument, 8 out of memory. */
+int oracle_gen_rmat(int scale, uint64_t edge_factor, double a, double b, double c, uint64_t seed, int threads,
+                    uint64_t* out);
+
+/* Entries as a symmetric pattern .mtx (1-based "max min" lines, as given):
+ * the reference binary's input. 0 ok, 2 I/O error, 8 out of memory. */
+int oracle_write_mtx(const char* path, uint64_t num_nodes, const uint64_t* entries, uint64_t n_entries);
+
 #ifdef __cplusplus
 }
 #endif

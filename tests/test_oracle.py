@@ -113,3 +113,14 @@ def test_reference_binary_rmat18_pins_oracle():
     oracle._lib.oracle_tribit_blocks.restype = ctypes.c_uint64
     oracle._lib.oracle_tribit_blocks.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
     assert oracle._lib.oracle_tribit_blocks(f.ctypes.data, f.size) == rec["blocks_of_threads"]
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(8, 16, 1), (12, 4, 7), (16, 16, 24)])
+def test_oracle_rmat_generator_matches_product(scale, ef, seed):
+    # The benchmark's reference arm generates its graph with the oracle's own
+    # R-MAT restatement (it must not load the product library); both must give
+    # the same words, for any host thread count.
+    import tribit_b200 as tb
+    want = tb.gen_rmat(scale, ef, seed=seed)
+    for threads in (1, 3, 8):
+        np.testing.assert_array_equal(oracle.gen_rmat(scale, ef, seed=seed, threads=threads), want)

@@ -91,12 +91,13 @@ _decl("tribit_model_gradients", ctypes.c_int, _p, _p, _p, _u64, _p, ctypes.POINT
 _decl("tribit_model_train", ctypes.c_int, _p, _p, _p, _u64, _u32, _u32, ctypes.c_float, _u64,
       ctypes.POINTER(ctypes.c_float))
 _decl("tribit_block_features", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
+_decl("tribit_block_variants", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
 _decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POINTER(_u64),
       ctypes.POINTER(ctypes.c_float))
 class Tuning(ctypes.Structure):
     """tribit_tuning: launch parameters of the counting kernels."""
     _fields_ = [("ctas_per_sm", ctypes.c_int), ("piece_width", _u32), ("tile_min_nnz", ctypes.c_float),
-                ("count_ms", ctypes.c_float)]
+                ("count_ms", ctypes.c_float), ("merge_ratio", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -206,8 +207,12 @@ class Counter:
         _check(lib.tribit_get_tuning(self._h, ctypes.byref(t)), self._h)
         return t
 
-    def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 64.0):
-        t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0)
+    def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 64.0,
+                   merge_ratio: float | None = None):
+        """merge_ratio None keeps the context's current plain-rule merge threshold."""
+        if merge_ratio is None:
+            merge_ratio = self.tuning().merge_ratio
+        t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0, merge_ratio)
         _check(lib.tribit_set_tuning(self._h, ctypes.byref(t)), self._h)
 
     def set_tile_engine(self, engine: str):
@@ -278,6 +283,14 @@ class Counter:
         _check(lib.tribit_block_features(self._h, None, 0, ctypes.byref(nrb)), self._h)
         out = np.zeros((nrb.value, 16), dtype=np.float32)
         _check(lib.tribit_block_features(self._h, out.ctypes.data, out.size, ctypes.byref(nrb)), self._h)
+        return out
+
+    def block_variants(self) -> np.ndarray:
+        """The dispatcher's variant index (see VARIANTS) of every 32-row block."""
+        nrb = _u64()
+        _check(lib.tribit_block_variants(self._h, None, 0, ctypes.byref(nrb)), self._h)
+        out = np.zeros(nrb.value, dtype=np.uint8)
+        _check(lib.tribit_block_variants(self._h, out.ctypes.data, out.size, ctypes.byref(nrb)), self._h)
         return out
 
     def block_times(self, variant: str):

@@ -319,6 +319,19 @@ tribit_status tribit_capture_count(tribit_context* c) {
   });
 }
 
+tribit_status tribit_block_variants(tribit_context* c, uint8_t* out, uint64_t cap, uint64_t* num_row_blocks) {
+  if (!c || !c->prepared || !num_row_blocks) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    DeviceGuard dg(c->device);
+    const uint64_t nrb = c->sched.num_row_blocks;
+    *num_row_blocks = nrb;
+    if (!out) return;
+    if (cap < nrb) throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "output buffer too small");
+    if (nrb) TB_CUDA(cudaMemcpyAsync(out, c->sched.variant_of, nrb, cudaMemcpyDeviceToHost, c->st));
+    TB_CUDA(cudaStreamSynchronize(c->st));
+  });
+}
+
 tribit_status tribit_read_batch_counts(tribit_context* c, uint64_t* out, uint32_t num_graphs) {
   if (!c || !c->prepared || !out || num_graphs != c->num_graphs || num_graphs == 0) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
@@ -334,17 +347,20 @@ tribit_status tribit_get_tuning(tribit_context* c, tribit_tuning* t) {
   t->piece_width = c->piece_width;
   t->tile_min_nnz = c->tile_min_nnz;
   t->count_ms = 0.f;
+  t->merge_ratio = c->merge_ratio;
   return TRIBIT_OK;
 }
 
 tribit_status tribit_set_tuning(tribit_context* c, const tribit_tuning* t) {
   if (!c || !t || t->ctas_per_sm < 0 || t->ctas_per_sm > 32 || t->piece_width < tb::kMinPieceWidth ||
-      t->piece_width % 32 != 0 || t->piece_width > 4096 || !(t->tile_min_nnz >= 0.f))
+      t->piece_width % 32 != 0 || t->piece_width > 4096 || !(t->tile_min_nnz >= 0.f) ||
+      !(t->merge_ratio >= 0.f))
     return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     c->ctas_per_sm = t->ctas_per_sm;
     c->piece_width = t->piece_width;
     c->tile_min_nnz = t->tile_min_nnz;
+    c->merge_ratio = t->merge_ratio;
     if (c->prepared) {
       DeviceGuard dg(c->device);
       tb::apply_dispatch(c, c->st);
@@ -390,6 +406,7 @@ tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* b
   static const float kTile[] = {64.f, 1e30f};
   tribit_tuning cur{}, found{};
   found.count_ms = 1e30f;
+  cur.merge_ratio = c->merge_ratio;  // the plain rule's merge threshold stays as set
   for (int ctas : kCtas)
     for (uint32_t w : kWidths)
       for (float tile : kTile) {

@@ -33,6 +33,7 @@ struct tribit_context {
   uint32_t piece_width = 64;
   int tile_engine = TRIBIT_TILES_TCGEN05;  // measured faster than mma.sync on dense tiles
   float tile_min_nnz = 64.f;
+  float merge_ratio = tb::kDefaultMergeRatio;
   uint32_t tile_wait_polls = 0;        // tcgen05 tiles' bounded mbarrier wait (0: the default budget)
   uint32_t num_graphs = 0;             // batch size of the prepared input (0: single graph)
   cudaGraph_t graph = nullptr;         // captured counting launch (tribit_capture_count)

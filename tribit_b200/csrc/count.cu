@@ -1517,7 +1517,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
 // Row-block features (one warp per row block) and the plain dispatcher's
 // choice. Features are log-scaled so the learned dispatcher sees O(1) inputs.
 __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restrict__ feat,
-                           uint8_t* __restrict__ variant_of, int full, float tile_min_nnz) {
+                           uint8_t* __restrict__ variant_of, int full, float tile_min_nnz, float merge_ratio) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1595,10 +1595,17 @@ __global__ void k_features(GraphView g, uint32_t nrb, int mode, float* __restric
       // share one narrow column range and are dense in it (at least 1/8 of
       // the 32 x 32 * span cells set, and tile_min_nnz edges): on disjoint
       // cliques tiles beat the sweeps, on sparse small graphs (1-2 % dense)
-      // they lose. The bitmap sweep everywhere else.
+      // they lose. Otherwise the sorted-list merge where the neighbours' bit
+      // rows average at least merge_ratio times the block's own (wb / nnz
+      // against nb / rows; needs the neighbour-side pass): the power-law
+      // case, where the merge's hub pass walks u's short tail against a long,
+      // staged row of v instead of probing every block of v. The bitmap sweep
+      // everywhere else (rows and neighbours of similar length).
       uint8_t var = TRIBIT_VARIANT_BITMAP;
       if (span > 0.f && span <= (float)kTileMaxK && nnz >= tile_min_nnz && nnz >= span * (1024.f / kTileMinDensityInv))
         var = TRIBIT_VARIANT_MMA;
+      else if (full && rows > 0.f && nnz > 0.f && wb >= merge_ratio * nnz * (nb / rows))
+        var = TRIBIT_VARIANT_MERGE;
       if (mode == TRIBIT_DISPATCH_BITMAP) var = TRIBIT_VARIANT_BITMAP;
       if (mode == TRIBIT_DISPATCH_MERGE) var = TRIBIT_VARIANT_MERGE;
       if (mode == TRIBIT_DISPATCH_MMA) var = TRIBIT_VARIANT_MMA;
@@ -2107,7 +2114,7 @@ void compute_features(const GraphView& g, Schedule& s, int mode, bool full_featu
   if (nrb == 0) return;
   const unsigned blocks = (unsigned)std::min<uint64_t>(ceil_div<uint64_t>(nrb, 8), 148ull * 16);
   k_features<<<blocks, 256, 0, st>>>(g, nrb, mode, s.features, s.variant_of, full_features ? 1 : 0,
-                                     s.tile_min_nnz);
+                                     s.tile_min_nnz, s.merge_ratio);
   TB_LAUNCH_CHECK();
 }
 

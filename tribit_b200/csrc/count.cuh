@@ -25,6 +25,9 @@ constexpr int kNumFeatures = 16;
 constexpr int kTileMaxK = 64;  // bit-tile variant: row blocks spanning at most this many column blocks
 constexpr int kFeatSpan = 13;  // feature index of log2(1 + column-block span)
 constexpr uint32_t kMinPieceWidth = 32;  // piece_width is a multiple of 32, at least this
+// Plain dispatcher: a row block goes to the merge variant when its neighbours'
+// bit rows average at least this many times its own rows' length.
+constexpr float kDefaultMergeRatio = 2.f;
 
 struct Schedule {
   uint32_t num_row_blocks = 0;
@@ -63,6 +66,7 @@ struct Schedule {
   bool hubs_active = false;        // set by build_pieces
   uint32_t piece_width = 64;       // neighbours per piece (tuned)
   float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
+  float merge_ratio = kDefaultMergeRatio;  // plain dispatcher: merge where neighbours' bit rows are this much longer
   int tile_engine = TRIBIT_TILES_TCGEN05;  // bit-tile product: tcgen05 kind::i8 or b1 mma.sync
   const void* model = nullptr;     // device MLP parameters for learned dispatch
 };

@@ -341,8 +341,11 @@ void apply_dispatch(tribit_context* c, cudaStream_t st) {
   const int mode = c->opts.dispatch;
   c->sched.piece_width = c->piece_width;
   c->sched.tile_min_nnz = c->tile_min_nnz;
+  c->sched.merge_ratio = c->merge_ratio;
   c->sched.tile_engine = c->tile_engine;
-  c->sched.hubs = mode == TRIBIT_DISPATCH_LEARNED || mode == TRIBIT_DISPATCH_MERGE;  // only merge blocks use them
+  // Only merge blocks use the hub lists; the plain rule picks merge blocks
+  // from the neighbour-side features, so it reads the full set too.
+  c->sched.hubs = mode == TRIBIT_DISPATCH_LEARNED || mode == TRIBIT_DISPATCH_MERGE || mode == TRIBIT_DISPATCH_PLAIN;
   drop_graph(c);
   if (mode == TRIBIT_DISPATCH_LEARNED) {
     require_model(c);
@@ -350,7 +353,7 @@ void apply_dispatch(tribit_context* c, cudaStream_t st) {
     model_dispatch(c->model, c->sched.features, c->sched.num_row_blocks, c->sched.variant_of, st);
     build_pieces(c->prep.view, c->sched, st);
   } else {
-    build_schedule(c->prep.view, c->sched, mode, false, st);
+    build_schedule(c->prep.view, c->sched, mode, mode == TRIBIT_DISPATCH_PLAIN, st);
   }
 }
 
