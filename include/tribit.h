@@ -97,6 +97,9 @@ typedef struct tribit_result {
   uint32_t count_kernels;     /* kernels one counting launch issues */
   uint32_t hub_edges;         /* edges the merge variant counts by walking u's tail against the
                                  staged row of v (the hub pass) */
+  float load_ms;              /* tribit_count_mtx / tribit_count_loaded: wall time of reading the
+                                 file into device memory (tribit_load_mtx); else 0 */
+  uint32_t load_gpu_parse;    /* 1 when the GPU parsed the file, 0 when the host grammar did */
 } tribit_result;
 
 typedef struct tribit_context tribit_context;
@@ -177,6 +180,22 @@ tribit_status tribit_read_batch_counts(tribit_context* ctx, uint64_t* triangles_
  * released with tribit_free_host. */
 tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, uint64_t** entries, uint64_t* n_entries);
 void tribit_free_host(void* p);
+/* Reads a Matrix Market file into the context's device memory, with the
+ * semantics of tribit_read_mtx (the same entries in the same order), for
+ * tribit_count_loaded. The file's bytes are read by host threads into pinned
+ * buffers and copied to the GPU piece by piece (each piece's copy overlaps
+ * the reading of the next), and the GPU parses the text: the reference's
+ * read_mtx (tribit.cu:228-269) parses on one host thread. A file with any
+ * line outside the common form "id blanks id [blanks number]*" (blank lines
+ * allowed) is parsed by the host's exact grammar instead. The loaded graph
+ * stays until the next load or tribit_destroy. */
+tribit_status tribit_load_mtx(tribit_context* ctx, const char* path, uint64_t* num_nodes, uint64_t* n_entries);
+/* Counts the graph of the latest tribit_load_mtx (as tribit_count_edges_device). */
+tribit_status tribit_count_loaded(tribit_context* ctx, tribit_result* out);
+/* Copies the loaded entries (n_entries words) to host memory; out may be NULL
+ * to query the count. */
+tribit_status tribit_loaded_entries(tribit_context* ctx, uint64_t* out, uint64_t cap, uint64_t* n_entries);
+/* tribit_load_mtx + tribit_count_loaded. */
 tribit_status tribit_count_mtx(tribit_context* ctx, const char* path, tribit_result* out);
 
 /* ---- batches ----------------------------------------------------------- */

@@ -54,7 +54,8 @@ class _Result(ctypes.Structure):
     _fields_ = [("triangles", _u64), ("num_nodes", _u64), ("entries", _u64), ("edges", _u64),
                 ("blocks_of_threads", _u64), ("row_blocks", _u64), ("row_blocks_by_variant", _u64 * 3),
                 ("h2d_ms", ctypes.c_float), ("preprocess_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
-                ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("hub_edges", _u32)]
+                ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("hub_edges", _u32),
+                ("load_ms", ctypes.c_float), ("load_gpu_parse", _u32)]
 
 
 def _decl(name, res, *args):
@@ -79,6 +80,9 @@ _decl("tribit_read_count", ctypes.c_int, _p, ctypes.POINTER(_Result))
 _decl("tribit_read_mtx", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_p), ctypes.POINTER(_u64))
 _decl("tribit_free_host", None, _p)
 _decl("tribit_count_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
+_decl("tribit_load_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64))
+_decl("tribit_count_loaded", ctypes.c_int, _p, ctypes.POINTER(_Result))
+_decl("tribit_loaded_entries", ctypes.c_int, _p, _p, _u64, ctypes.POINTER(_u64))
 _decl("tribit_count_batch", ctypes.c_int, _p, _p, _p, _p, _u32, _p, ctypes.POINTER(_Result))
 _decl("tribit_model_load", ctypes.c_int, _p, ctypes.c_char_p)
 _decl("tribit_model_save", ctypes.c_int, _p, ctypes.c_char_p)
@@ -151,12 +155,14 @@ class Result:
     total_ms: float
     count_kernels: int
     hub_edges: int
+    load_ms: float = 0.0
+    load_gpu_parse: int = 0
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         return cls(r.triangles, r.num_nodes, r.entries, r.edges, r.blocks_of_threads, r.row_blocks,
                    tuple(r.row_blocks_by_variant), r.h2d_ms, r.preprocess_ms, r.kernel_ms, r.total_ms,
-                   r.count_kernels, r.hub_edges)
+                   r.count_kernels, r.hub_edges, r.load_ms, r.load_gpu_parse)
 
 
 def _entries(a) -> np.ndarray:
@@ -331,6 +337,25 @@ class Counter:
         r = _Result()
         _check(lib.tribit_count_mtx(self._h, path.encode(), ctypes.byref(r)), self._h)
         return Result._from(r)
+
+    def load_mtx(self, path: str):
+        """tribit_load_mtx: the file parsed into device memory -> (num_nodes, entries)."""
+        n, e = _u64(), _u64()
+        _check(lib.tribit_load_mtx(self._h, str(path).encode(), ctypes.byref(n), ctypes.byref(e)), self._h)
+        return n.value, e.value
+
+    def count_loaded(self) -> Result:
+        r = _Result()
+        _check(lib.tribit_count_loaded(self._h, ctypes.byref(r)), self._h)
+        return Result._from(r)
+
+    def loaded_entries(self) -> np.ndarray:
+        cnt = _u64()
+        _check(lib.tribit_loaded_entries(self._h, None, 0, ctypes.byref(cnt)), self._h)
+        out = np.zeros(cnt.value, dtype=np.uint64)
+        _check(lib.tribit_loaded_entries(self._h, out.ctypes.data if out.size else None, out.size,
+                                         ctypes.byref(cnt)), self._h)
+        return out
 
     def count_batch(self, entries, offsets, num_nodes):
         """Counts len(num_nodes) graphs in one launch; returns (counts, Result)."""

@@ -211,6 +211,10 @@ void tribit_destroy(tribit_context* c) {
     DeviceGuard dg(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
     c->arena.release();
+    c->text_arena.release();
+    c->load_arena.release();
+    for (auto& p : c->pinned)
+      if (p) cudaFreeHost(p);
     tb::drop_graph(c);
     c->train_arena.release();
     c->timing_arena.release();
@@ -457,17 +461,6 @@ tribit_status tribit_read_count(tribit_context* c, tribit_result* out) {
       fill_schedule_stats(c, out);
     }
   });
-}
-
-tribit_status tribit_count_mtx(tribit_context* c, const char* path, tribit_result* out) {
-  if (!c || !path) return TRIBIT_ERR_INVALID_ARGUMENT;
-  uint64_t n = 0, ne = 0;
-  uint64_t* e = nullptr;
-  tribit_status s = tribit_read_mtx(path, &n, &e, &ne);
-  if (s != TRIBIT_OK) return s;
-  s = tribit_count_edges(c, e, ne, n, out);
-  tribit_free_host(e);
-  return s;
 }
 
 tribit_status tribit_count_batch(tribit_context* c, const uint64_t* entries, const uint64_t* entry_offsets,

@@ -39,6 +39,16 @@ struct tribit_context {
   cudaGraph_t graph = nullptr;         // captured counting launch (tribit_capture_count)
   cudaGraphExec_t graph_exec = nullptr;
   tb::DeviceModel model{};
+  // Matrix Market ingest (tribit_load_mtx): the file's text and its segment
+  // counts, the parsed entries, and two pinned upload buffers.
+  tb::Arena text_arena;
+  tb::Arena load_arena;
+  void* pinned[2] = {nullptr, nullptr};
+  const uint64_t* loaded_entries = nullptr;
+  uint64_t loaded_E = 0, loaded_n = 0;
+  bool loaded = false;
+  float load_ms = 0.f;
+  uint32_t load_gpu_parse = 0;
   tb::Arena train_arena;               // training batches and activations
   tb::Arena timing_arena;              // per-row-block cycle counters
   std::string err;

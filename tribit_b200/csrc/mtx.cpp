@@ -28,6 +28,7 @@
 #include <thread>
 #include <vector>
 
+#include "mtx.h"
 #include "tribit.h"
 
 namespace {
@@ -218,25 +219,9 @@ size_t parse_strict_fast(const char* p, const char* end, uint64_t* out) {
 
 }  // namespace
 
-extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, uint64_t** entries,
-                                         uint64_t* n_entries) {
-  if (!path || !num_nodes || !entries || !n_entries) return TRIBIT_ERR_INVALID_ARGUMENT;
-  *entries = nullptr;
-  *n_entries = 0;
-  Mapped m;
-  m.fd = open(path, O_RDONLY);
-  if (m.fd < 0) return TRIBIT_ERR_IO;
-  struct stat sb;
-  if (fstat(m.fd, &sb) != 0) return TRIBIT_ERR_IO;
-  m.len = (size_t)sb.st_size;
-  if (m.len > 0) {
-    void* q = mmap(nullptr, m.len, PROT_READ, MAP_PRIVATE, m.fd, 0);
-    if (q == MAP_FAILED) return TRIBIT_ERR_IO;
-    m.p = (const char*)q;
-    madvise(q, m.len, MADV_SEQUENTIAL);
-  }
-  const char* p = m.p;
-  const char* end = m.p + m.len;
+namespace tb {
+
+tribit_status mtx_header(const char* p, const char* end, const char** body, uint64_t* num_nodes, uint64_t* nnz) {
   // Banner line (tribit.cu:232), then lines starting with '%' (tribit.cu:234-235).
   const char* nl = p < end ? (const char*)std::memchr(p, '\n', (size_t)(end - p)) : nullptr;
   p = nl ? nl + 1 : end;
@@ -265,6 +250,37 @@ extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, 
   }
   if (dims[0] != dims[1]) return TRIBIT_ERR_NOT_SQUARE;
   *num_nodes = dims[0];
+  *nnz = dims[2];
+  *body = p;
+  return TRIBIT_OK;
+}
+
+}  // namespace tb
+
+extern "C" tribit_status tribit_read_mtx(const char* path, uint64_t* num_nodes, uint64_t** entries,
+                                         uint64_t* n_entries) {
+  if (!path || !num_nodes || !entries || !n_entries) return TRIBIT_ERR_INVALID_ARGUMENT;
+  *entries = nullptr;
+  *n_entries = 0;
+  Mapped m;
+  m.fd = open(path, O_RDONLY);
+  if (m.fd < 0) return TRIBIT_ERR_IO;
+  struct stat sb;
+  if (fstat(m.fd, &sb) != 0) return TRIBIT_ERR_IO;
+  m.len = (size_t)sb.st_size;
+  if (m.len > 0) {
+    void* q = mmap(nullptr, m.len, PROT_READ, MAP_PRIVATE, m.fd, 0);
+    if (q == MAP_FAILED) return TRIBIT_ERR_IO;
+    m.p = (const char*)q;
+    madvise(q, m.len, MADV_SEQUENTIAL);
+  }
+  const char* p = nullptr;
+  const char* end = m.p + m.len;
+  uint64_t dims[3];
+  {
+    const tribit_status hs = tb::mtx_header(m.p, end, &p, num_nodes, &dims[2]);
+    if (hs != TRIBIT_OK) return hs;
+  }
 
   // Entries: parallel strict parse, else the exact grammar.
   std::vector<uint64_t> all;
