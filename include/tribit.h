@@ -100,6 +100,9 @@ typedef struct tribit_result {
   float load_ms;              /* tribit_count_mtx / tribit_count_loaded: wall time of reading the
                                  file into device memory (tribit_load_mtx); else 0 */
   uint32_t load_gpu_parse;    /* 1 when the GPU parsed the file, 0 when the host grammar did */
+  uint32_t stream_ranges;     /* tribit_count_edges: 1 when the graph fit the device budget, else the
+                                 rank ranges it was counted in (see tribit_set_device_budget) */
+  uint32_t stream_tasks;      /* counts of range pairs those ranges took (1 in one piece) */
 } tribit_result;
 
 typedef struct tribit_context tribit_context;
@@ -118,9 +121,23 @@ const char* tribit_last_error(const tribit_context* ctx);
 const char* tribit_version(void);
 
 /* ---- single graph ------------------------------------------------------ */
-/* Host entries -> exact count (H2D copy, preprocessing, counting, D2H). */
+/* Host entries -> exact count (H2D copy, preprocessing, counting, D2H).
+ * A graph whose device buffers exceed the context's device budget (all the
+ * memory the device has free, unless tribit_set_device_budget says less) is
+ * counted in pieces: its entries are streamed through the GPU to rank them
+ * and sort them into host buckets by rank range, and each pair of ranges is
+ * then counted on the device (result.stream_ranges > 1). The reference splits
+ * a graph too large for a GPU into partitions and tasks of at most 1e9
+ * entries over several GPUs (src/multi_gpu/src/main.rs:98-220). Such a count
+ * leaves no prepared graph in the context (tribit_launch_count then fails). */
 tribit_status tribit_count_edges(tribit_context* ctx, const uint64_t* entries, uint64_t n_entries, uint64_t num_nodes,
                                  tribit_result* out);
+/* Device memory (bytes) a one-piece tribit_count_edges of n_entries entries on
+ * num_nodes vertices takes in this context (its arena, staged input included). */
+tribit_status tribit_device_bytes(tribit_context* ctx, uint64_t n_entries, uint64_t num_nodes, uint64_t* bytes);
+/* Caps the device memory later tribit_count_edges calls of this context may
+ * use (bytes; 0 = what the device has free at the call). */
+tribit_status tribit_set_device_budget(tribit_context* ctx, uint64_t bytes);
 /* Same with the entries already in device memory. */
 tribit_status tribit_count_edges_device(tribit_context* ctx, const uint64_t* d_entries, uint64_t n_entries,
                                         uint64_t num_nodes, tribit_result* out);

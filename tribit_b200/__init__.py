@@ -55,7 +55,8 @@ class _Result(ctypes.Structure):
                 ("blocks_of_threads", _u64), ("row_blocks", _u64), ("row_blocks_by_variant", _u64 * 3),
                 ("h2d_ms", ctypes.c_float), ("preprocess_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("hub_edges", _u32),
-                ("load_ms", ctypes.c_float), ("load_gpu_parse", _u32)]
+                ("load_ms", ctypes.c_float), ("load_gpu_parse", _u32), ("stream_ranges", _u32),
+                ("stream_tasks", _u32)]
 
 
 def _decl(name, res, *args):
@@ -73,6 +74,8 @@ _decl("tribit_status_string", ctypes.c_char_p, ctypes.c_int)
 _decl("tribit_last_error", ctypes.c_char_p, _p)
 _decl("tribit_version", ctypes.c_char_p)
 _decl("tribit_count_edges", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
+_decl("tribit_set_device_budget", ctypes.c_int, _p, _u64)
+_decl("tribit_device_bytes", ctypes.c_int, _p, _u64, _u64, ctypes.POINTER(_u64))
 _decl("tribit_count_edges_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
 _decl("tribit_prepare_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
 _decl("tribit_launch_count", ctypes.c_int, _p)
@@ -157,12 +160,14 @@ class Result:
     hub_edges: int
     load_ms: float = 0.0
     load_gpu_parse: int = 0
+    stream_ranges: int = 0
+    stream_tasks: int = 0
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         return cls(r.triangles, r.num_nodes, r.entries, r.edges, r.blocks_of_threads, r.row_blocks,
                    tuple(r.row_blocks_by_variant), r.h2d_ms, r.preprocess_ms, r.kernel_ms, r.total_ms,
-                   r.count_kernels, r.hub_edges, r.load_ms, r.load_gpu_parse)
+                   r.count_kernels, r.hub_edges, r.load_ms, r.load_gpu_parse, r.stream_ranges, r.stream_tasks)
 
 
 def _entries(a) -> np.ndarray:
@@ -314,6 +319,17 @@ class Counter:
         r = _Result()
         _check(lib.tribit_count_edges(self._h, e.ctypes.data, e.size, int(num_nodes), ctypes.byref(r)), self._h)
         return Result._from(r)
+
+    def set_device_budget(self, nbytes: int):
+        """Device memory later count_edges calls may use (0 = what is free); a
+        graph needing more is counted in rank ranges (Result.stream_ranges > 1)."""
+        _check(lib.tribit_set_device_budget(self._h, int(nbytes)), self._h)
+
+    def device_bytes(self, n_entries: int, num_nodes: int) -> int:
+        """Device memory a one-piece count_edges of this size takes."""
+        b = _u64()
+        _check(lib.tribit_device_bytes(self._h, int(n_entries), int(num_nodes), ctypes.byref(b)), self._h)
+        return b.value
 
     def count_edges_device(self, ptr: int, n_entries: int, num_nodes: int) -> Result:
         r = _Result()

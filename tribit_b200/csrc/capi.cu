@@ -120,6 +120,34 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
   }
 }
 
+}  // namespace
+
+namespace tb {
+
+size_t call_bytes(tribit_context* c, uint64_t E, uint64_t n, int order, bool stage) {
+  tb::PrepInput in;
+  in.E = E;
+  in.n = n;
+  in.order = order;
+  CallLayout L;
+  layout(c, true, in, stage, 0, &L);
+  return c->arena.used();
+}
+
+void count_device_input(tribit_context* c, const uint64_t* d_entries, uint64_t E, uint64_t n, int order,
+                        tribit_result* res) {
+  tb::PrepInput in;
+  in.entries = d_entries;
+  in.E = E;
+  in.n = n;
+  in.order = order;
+  run_call(c, in, nullptr, nullptr, nullptr, 0, true, res);
+}
+
+}  // namespace tb
+
+namespace {
+
 void fill_schedule_stats(tribit_context* c, tribit_result* res) {
   uint32_t lens[TRIBIT_NUM_VARIANTS], hub_edges = 0;
   TB_CUDA(cudaMemcpyAsync(lens, c->sched.list_len, sizeof lens, cudaMemcpyDeviceToHost, c->st));
@@ -212,6 +240,7 @@ void tribit_destroy(tribit_context* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     c->arena.release();
     c->text_arena.release();
+    c->stream_arena.release();
     c->load_arena.release();
     for (auto& p : c->pinned)
       if (p) cudaFreeHost(p);
@@ -246,14 +275,24 @@ tribit_status tribit_count_edges(tribit_context* c, const uint64_t* entries, uin
                                  tribit_result* out) {
   if (!c || (!entries && n_entries)) return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
+    if (entries && tb::count_streamed_if_needed(c, entries, n_entries, num_nodes, out)) return;
     tb::PrepInput in;
     in.E = n_entries;
     in.n = num_nodes;
     in.order = c->opts.order;
     static const uint64_t dummy = 0;
     run_call(c, in, entries ? entries : &dummy, nullptr, nullptr, 0, true, out);
-    if (out) fill_schedule_stats(c, out);
+    if (out) {
+      fill_schedule_stats(c, out);
+      out->stream_ranges = 1;
+      out->stream_tasks = 1;
+    }
   });
+}
+
+tribit_status tribit_device_bytes(tribit_context* c, uint64_t n_entries, uint64_t num_nodes, uint64_t* bytes) {
+  if (!c || !bytes) return TRIBIT_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] { *bytes = tb::call_bytes(c, n_entries, num_nodes, c->opts.order, true); });
 }
 
 tribit_status tribit_count_edges_device(tribit_context* c, const uint64_t* d_entries, uint64_t n_entries,

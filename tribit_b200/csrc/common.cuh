@@ -67,6 +67,16 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = t > v ? t : v;
+  }
+  return v;
+}
+
 // Runs fn() once per CUDA device (the current one when called), for settings
 // such as cudaFuncSetAttribute that apply per device. Thread-safe; a call whose
 // fn throws leaves the device unmarked, so a later call retries it.

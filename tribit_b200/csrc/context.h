@@ -49,6 +49,10 @@ struct tribit_context {
   bool loaded = false;
   float load_ms = 0.f;
   uint32_t load_gpu_parse = 0;
+  // Device memory the context may use (tribit_set_device_budget; 0: what the
+  // device has free); graphs needing more are counted in rank ranges.
+  uint64_t device_budget = 0;
+  tb::Arena stream_arena;              // streamed counts: degrees, ranks, row counts, piece buffers
   tb::Arena train_arena;               // training batches and activations
   tb::Arena timing_arena;              // per-row-block cycle counters
   std::string err;
@@ -92,6 +96,20 @@ tribit_status guarded(tribit_context* ctx, F&& body) {
 // Rebuilds the context's schedule for its dispatch mode (learned mode runs the
 // MLP over full features) with its tuned piece width and tile threshold.
 void apply_dispatch(tribit_context* c, cudaStream_t st);
+
+// Device bytes of the context's arena for one count of E entries on n
+// vertices in `order` (stage: host input staged on the device).
+size_t call_bytes(tribit_context* c, uint64_t E, uint64_t n, int order, bool stage);
+// One count of E device entries on n vertices in `order` with the context's
+// dispatcher (tribit_count_edges_device with an explicit order).
+void count_device_input(tribit_context* c, const uint64_t* d_entries, uint64_t E, uint64_t n, int order,
+                        tribit_result* res);
+// Counts host entries in rank ranges when their buffers exceed the device
+// budget (stream.cu). Returns false, doing nothing, when they fit.
+bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t E, uint64_t n, tribit_result* res);
+// Copies bytes of host memory to device memory through the context's two
+// pinned buffers (host threads fill one while the other's copy runs).
+void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst);
 
 // Launch configuration of the context's counting kernels.
 inline CountConfig count_config(const tribit_context* c) {

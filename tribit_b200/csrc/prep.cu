@@ -492,6 +492,28 @@ void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t
 
 }  // namespace
 
+RankBuffers take_rank_buffers(Arena& ar, uint64_t n) {
+  RankBuffers b;
+  b.vk = ar.take<uint32_t>(n ? n : 1);
+  b.vk2 = ar.take<uint32_t>(n ? n : 1);
+  b.vv = ar.take<uint32_t>(n ? n : 1);
+  b.vv2 = ar.take<uint32_t>(n ? n : 1);
+  b.tmp = take_radix_temp(ar, n);
+  return b;
+}
+
+void rank_vertices(const uint32_t* deg, uint64_t n, uint64_t E, const RankBuffers& b, uint32_t* rank, cudaStream_t st) {
+  if (n == 0) return;
+  int dbits = bits_for(2 * E + 2);
+  if (dbits > 32) dbits = 32;
+  k_vertex_keys<<<grid_for(n), kThreads, 0, st>>>(deg, n, nullptr, 0, 32, b.vk, b.vv);
+  TB_LAUNCH_CHECK();
+  uint32_t* sorted_ids = nullptr;
+  radix_sort<uint32_t, uint32_t, true>(b.vk, b.vk2, b.vv, b.vv2, n, dbits, b.tmp, st, &sorted_ids);
+  k_rank_scatter<<<grid_for(n), kThreads, 0, st>>>(sorted_ids, n, rank, nullptr, 0, nullptr);
+  TB_LAUNCH_CHECK();
+}
+
 void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* out) {
   const uint64_t n = in.n, E = in.E;
   if (n > 0xffffffffull || E > 0xfffffffeull)

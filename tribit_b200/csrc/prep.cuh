@@ -12,6 +12,7 @@
 
 #include "arena.h"
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace tb {
 
@@ -81,5 +82,15 @@ struct Prepared {
 // Lays out (measuring arena) or lays out and launches (real arena) the whole
 // preprocessing pipeline on stream st. Stats are zeroed here.
 void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* out);
+
+// The (degree, id) rank order of n vertices from their degrees (E entries
+// counted them, which bounds a degree by 2E): rank[v] = position of v. The
+// buffers come from take_rank_buffers; launches only.
+struct RankBuffers {
+  uint32_t *vk = nullptr, *vk2 = nullptr, *vv = nullptr, *vv2 = nullptr;
+  RadixTemp tmp{};
+};
+RankBuffers take_rank_buffers(Arena& ar, uint64_t n);
+void rank_vertices(const uint32_t* deg, uint64_t n, uint64_t E, const RankBuffers& b, uint32_t* rank, cudaStream_t st);
 
 }  // namespace tb
