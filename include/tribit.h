@@ -215,6 +215,18 @@ tribit_status tribit_loaded_entries(tribit_context* ctx, uint64_t* out, uint64_t
 /* tribit_load_mtx + tribit_count_loaded. */
 tribit_status tribit_count_mtx(tribit_context* ctx, const char* path, tribit_result* out);
 
+/* ---- WebGraph BVGraph ---------------------------------------------------- */
+/* Reads a graph in WebGraph's BVGraph format (basename.properties,
+ * basename.graph and, when present, basename.offsets), the input of the
+ * reference's multi-GPU loader (src/multi_gpu/src/main.rs:88, the Rust
+ * webgraph crate), and folds every arc (src, dst), src != dst, to
+ * (min << 32) | max as that loader does (main.rs:142-161). Big-endian streams
+ * with gamma, delta, unary and zeta codes; with offsets the nodes are decoded
+ * in parallel. *entries is allocated with malloc (tribit_free_host). */
+tribit_status tribit_read_bvgraph(const char* basename, uint64_t* num_nodes, uint64_t** entries, uint64_t* n_entries);
+/* tribit_read_bvgraph + tribit_count_edges. */
+tribit_status tribit_count_bvgraph(tribit_context* ctx, const char* basename, tribit_result* out);
+
 /* ---- batches ----------------------------------------------------------- */
 /* num_graphs independent graphs in one persistent counting launch. Graph g's
  * entries are entries[entry_offsets[g] .. entry_offsets[g + 1]) with vertex

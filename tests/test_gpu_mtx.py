@@ -108,3 +108,17 @@ def test_errors(counter, tmp_path):
     assert ex.value.status == 4
     # the context stays usable
     check_file(counter, write(tmp_path, "ok.mtx", "%%MatrixMarket x\n3 3 3\n1 2\n2 3\n3 1\n"))
+
+
+def test_bvgraph_count_matches_oracle(counter, tmp_path):
+    # A WebGraph BVGraph (the reference multi-GPU loader's input format,
+    # src/multi_gpu/src/main.rs:88), written by the oracle's encoder, counted
+    # through tribit_count_bvgraph; its arcs are the oracle's entries.
+    from oracle import bvgraph as bv
+    from tests.test_bvgraph import structured_graph
+    g = structured_graph(6000, 11)
+    base = str(tmp_path / "web")
+    bv.write(base, g)
+    want = oracle.count(bv.entries(g), len(g))
+    r = counter.count_bvgraph(base)
+    assert (r.triangles, r.edges) == want

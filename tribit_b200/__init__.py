@@ -82,6 +82,9 @@ _decl("tribit_launch_count", ctypes.c_int, _p)
 _decl("tribit_read_count", ctypes.c_int, _p, ctypes.POINTER(_Result))
 _decl("tribit_read_mtx", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_p), ctypes.POINTER(_u64))
 _decl("tribit_free_host", None, _p)
+_decl("tribit_read_bvgraph", ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_p),
+      ctypes.POINTER(_u64))
+_decl("tribit_count_bvgraph", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
 _decl("tribit_count_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_Result))
 _decl("tribit_load_mtx", ctypes.c_int, _p, ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64))
 _decl("tribit_count_loaded", ctypes.c_int, _p, ctypes.POINTER(_Result))
@@ -373,6 +376,11 @@ class Counter:
                                          ctypes.byref(cnt)), self._h)
         return out
 
+    def count_bvgraph(self, basename: str) -> Result:
+        r = _Result()
+        _check(lib.tribit_count_bvgraph(self._h, str(basename).encode(), ctypes.byref(r)), self._h)
+        return Result._from(r)
+
     def count_batch(self, entries, offsets, num_nodes):
         """Counts len(num_nodes) graphs in one launch; returns (counts, Result)."""
         e = _entries(entries)
@@ -417,6 +425,27 @@ def read_mtx(path: str):
         lib.tribit_free_host(ctypes.c_void_p(addr))
         raise
     return n.value, arr
+
+
+def _host_words(ptr: int, count: int) -> np.ndarray:
+    """The library's malloc'd entry buffer as an array (freed with the array)."""
+    try:
+        buf = (ctypes.c_uint64 * max(count, 1)).from_address(ptr)
+        arr = np.frombuffer(buf, dtype=np.uint64, count=count)
+        weakref.finalize(arr, lib.tribit_free_host, ctypes.c_void_p(ptr))
+    except BaseException:
+        lib.tribit_free_host(ctypes.c_void_p(ptr))
+        raise
+    return arr
+
+
+def read_bvgraph(basename: str):
+    """Reads a WebGraph BVGraph (basename.properties / .graph / .offsets) -> (num_nodes, entries)."""
+    n = _u64()
+    ptr = _p()
+    cnt = _u64()
+    _check(lib.tribit_read_bvgraph(str(basename).encode(), ctypes.byref(n), ctypes.byref(ptr), ctypes.byref(cnt)))
+    return n.value, _host_words(ptr.value, cnt.value)
 
 
 def write_mtx(path: str, num_nodes: int, entries):

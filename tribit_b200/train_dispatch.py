@@ -57,14 +57,17 @@ def training_graphs(quick: bool):
     if quick:
         return [("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(4000, 103)), ("batch_s101", batch(64, 101)),
                 ("cliques_32x256", cliques(32, 256))]
-    return [("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)), ("planted_s103", planted(20000, 103)),
+    # RMAT at several scales: which variant wins a block shifts with the graph's size.
+    return [("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)), ("rmat20_s120", rmat(20, 120)),
+            ("rmat19_s119", rmat(19, 119)), ("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(20000, 103)),
             ("batch_s101", batch(1024, 101)), ("cliques_96x384", cliques(96, 384))]
 
 
-def holdout_graph(quick: bool):
+def holdout_graphs(quick: bool):
     if quick:
-        return "rmat17_s7", ("graph", 1 << 17, tb.gen_rmat(17, 16, seed=7))
-    return "rmat22_s7", ("graph", 1 << 22, tb.gen_rmat(22, 16, seed=7))
+        return [("rmat17_s7", ("graph", 1 << 17, tb.gen_rmat(17, 16, seed=7)))]
+    return [("rmat22_s7", ("graph", 1 << 22, tb.gen_rmat(22, 16, seed=7))),
+            ("rmat18_s181", ("graph", 1 << 18, tb.gen_rmat(18, 16, seed=181)))]
 
 
 def collect(item, repeats: int = 2):
@@ -99,14 +102,14 @@ def collect(item, repeats: int = 2):
     return x[keep], t[keep], x, t
 
 
-def plain_choice(x):
-    """The plain dispatcher's rule, restated on the features (for the regret table)."""
-    nnz = np.exp2(x[:, 1]) - 1
-    span = np.exp2(x[:, 13]) - 1
-    choice = np.full(x.shape[0], tb.VARIANTS.index("bitmap"))
-    mma = (span > 0.5) & (span <= 64.5) & (nnz >= 63.5) & (nnz >= span * 128.0 - 0.5)
-    choice[mma] = tb.VARIANTS.index("mma")
-    return choice
+def plain_choice(item):
+    """The plain dispatcher's choice of every row block (tribit_block_variants)."""
+    import torch
+    _, n, e = item
+    d = torch.from_numpy(e.view(np.int64)).cuda()
+    with tb.Counter(dispatch="plain") as c:
+        c.prepare_device(d.data_ptr(), d.numel(), n)
+        return c.block_variants().astype(np.int64)
 
 
 def learned_choice(pred, x):
@@ -162,32 +165,36 @@ def main():
     Y = np.concatenate(ys).astype(np.float32)
     norm = np.concatenate([X.mean(0), X.std(0) + 1e-3, Y.mean(0), Y.std(0) + 1e-3]).astype(np.float32)
 
-    hname, hitem = holdout_graph(args.quick)
-    _, hn, he = hitem
-    hx, ht, _, _ = collect(hitem)
     with tb.Counter() as c:
         c.model_init(norm, seed=args.seed)
         loss = c.model_train(X, Y, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed)
         os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
         c.save_model(args.out)
-        pred = c.model_predict(hx)
-    learned = learned_choice(pred, hx)
-    plain = plain_choice(hx)
-    rows = np.arange(ht.shape[0])
-    best = ht.min(1).sum()
-    report = {
-        "train_rows": int(X.shape[0]), "final_loss": loss, "holdout": hname,
-        "holdout_cost_ms": {"best": float(best) / 1e6, "plain": float(ht[rows, plain].sum()) / 1e6,
-                            "learned": float(ht[rows, learned].sum()) / 1e6,
-                            **{f"all_{v}": float(ht[:, i].sum()) / 1e6 for i, v in enumerate(tb.VARIANTS)}},
-        "learned_picks": dict(zip(tb.VARIANTS, np.bincount(learned, minlength=3).tolist())),
-        "plain_picks": dict(zip(tb.VARIANTS, np.bincount(plain, minlength=3).tolist())),
-    }
-    p_ms, p_tri, _ = timed_count(hn, he, "plain", args.out)
-    l_ms, l_tri, _ = timed_count(hn, he, "learned", args.out)
-    assert p_tri == l_tri
-    report["holdout_count_ms"] = {"plain": p_ms, "learned": l_ms}
-    print(json.dumps(report), flush=True)
+    print(json.dumps({"train_rows": int(X.shape[0]), "final_loss": loss}), flush=True)
+    for hname, hitem in holdout_graphs(args.quick):
+        _, hn, he = hitem
+        # every row block, so that the choices line up with the costs
+        _, _, hx, ht = collect(hitem)
+        with tb.Counter() as c:
+            c.load_model(args.out)
+            pred = c.model_predict(hx)
+        learned = learned_choice(pred, hx)
+        plain = plain_choice(hitem)
+        rows = np.arange(ht.shape[0])
+        best = ht.min(1).sum()
+        report = {
+            "holdout": hname,
+            "holdout_cost_ms": {"best": float(best) / 1e6, "plain": float(ht[rows, plain].sum()) / 1e6,
+                                "learned": float(ht[rows, learned].sum()) / 1e6,
+                                **{f"all_{v}": float(ht[:, i].sum()) / 1e6 for i, v in enumerate(tb.VARIANTS)}},
+            "learned_picks": dict(zip(tb.VARIANTS, np.bincount(learned, minlength=3).tolist())),
+            "plain_picks": dict(zip(tb.VARIANTS, np.bincount(plain, minlength=3).tolist())),
+        }
+        p_ms, p_tri, _ = timed_count(hn, he, "plain", args.out)
+        l_ms, l_tri, _ = timed_count(hn, he, "learned", args.out)
+        assert p_tri == l_tri
+        report["holdout_count_ms"] = {"plain": p_ms, "learned": l_ms}
+        print(json.dumps(report), flush=True)
 
 
 if __name__ == "__main__":
