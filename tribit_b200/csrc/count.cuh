@@ -60,6 +60,7 @@ struct Schedule {
   uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail
   uint32_t* wave_lo = nullptr;     // device: first row of each wave, then n
   uint32_t* wave_cnt = nullptr;    // device: pieces per (list, wave), scanned to positions
+  uint32_t* fill_cursor = nullptr; // device: next row block of the in-list fill
   uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
   uint32_t* hub_scan_tmp = nullptr;
   bool hubs = true;                // build the hub lists for merge row blocks
