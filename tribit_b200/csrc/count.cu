@@ -1230,7 +1230,10 @@ constexpr uint32_t kHubHashMul = TB_HUB_HASH_MUL;  // hashed hubs must save this
 constexpr uint32_t kHubHashMin = TB_HUB_HASH_MIN;  // ... plus this many blocks (0 / 0: no hashed hubs)
 constexpr uint32_t kHubWarpHash = kHubWarpSpan / 4;        // bit blocks: warp hash
 constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per CTA piece
-constexpr uint32_t kHubWarpPiece = 256;         // in-edges per warp piece
+#ifndef TB_HUB_WARP_PIECE
+#define TB_HUB_WARP_PIECE 256
+#endif
+constexpr uint32_t kHubWarpPiece = TB_HUB_WARP_PIECE;  // in-edges per warp piece
 #ifndef TB_HUB_WAVES
 #define TB_HUB_WAVES 32
 #endif
