@@ -22,7 +22,7 @@ def counter():
     c.close()
 
 
-def check_file(c, path, gpu_parse=True):
+def check_file(c, path, gpu_parse=True, count_status=0):
     st, n0, want = oracle.read_mtx(str(path))
     assert st == 0
     n1, host = tb.read_mtx(str(path))
@@ -30,6 +30,12 @@ def check_file(c, path, gpu_parse=True):
     n, e = c.load_mtx(str(path))
     assert (n, e) == (n0, len(want))
     np.testing.assert_array_equal(c.loaded_entries(), want)
+    if count_status:
+        # e.g. a '-' id: the grammar wraps it modulo 2^32, past num_nodes
+        with pytest.raises(tb.TribitError) as ex:
+            c.count_loaded()
+        assert ex.value.status == count_status
+        return None
     r = c.count_loaded()
     assert r.load_gpu_parse == int(gpu_parse)
     assert (r.triangles, r.edges) == oracle.count(want, n0)
@@ -88,15 +94,16 @@ def test_empty_and_header_only(counter, tmp_path):
     check_file(counter, write(tmp_path, "noline.mtx", "%%MatrixMarket matrix coordinate pattern general\n5 5 0"))
 
 
-@pytest.mark.parametrize("name,text", [
-    ("trailing_blank", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n1 2 \n2 3\n3 1\n"),
-    ("crlf", "%%MatrixMarket matrix coordinate pattern general\r\n4 4 3\r\n1 2\r\n2 3\r\n3 1\r\n"),
-    ("signed_id", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n1 -2\n2 3\n3 1\n"),
-    ("word_token", "%%MatrixMarket matrix coordinate pattern general\n4 4 4\n1 2\n2 3\nend\n3 1\n"),
-    ("eleven_digits", "%%MatrixMarket matrix coordinate pattern general\n4 4 2\n1 2\n00000000003 1\n"),
+@pytest.mark.parametrize("name,text,status", [
+    ("trailing_blank", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n1 2 \n2 3\n3 1\n", 0),
+    ("crlf", "%%MatrixMarket matrix coordinate pattern general\r\n4 4 3\r\n1 2\r\n2 3\r\n3 1\r\n", 0),
+    ("signed_id", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n1 -2\n2 3\n3 1\n", 5),
+    ("plus_id", "%%MatrixMarket matrix coordinate pattern general\n4 4 3\n+1 2\n2 3\n3 1\n", 0),
+    ("word_token", "%%MatrixMarket matrix coordinate pattern general\n4 4 4\n1 2\n2 3\nend\n3 1\n", 0),
+    ("eleven_digits", "%%MatrixMarket matrix coordinate pattern general\n4 4 2\n1 2\n00000000003 1\n", 0),
 ])
-def test_other_forms_take_the_host_grammar(counter, tmp_path, name, text):
-    check_file(counter, write(tmp_path, name + ".mtx", text), gpu_parse=False)
+def test_other_forms_take_the_host_grammar(counter, tmp_path, name, text, status):
+    check_file(counter, write(tmp_path, name + ".mtx", text), gpu_parse=False, count_status=status)
 
 
 def test_errors(counter, tmp_path):

@@ -241,6 +241,8 @@ float ms_since(std::chrono::steady_clock::time_point t0) {
 
 void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst) {
   ensure_pinned(c);
+  // Copies of an earlier call may still read the pinned buffers.
+  TB_CUDA(cudaStreamSynchronize(c->copy_st));
   const size_t piece = kPieceWords * sizeof(uint64_t);
   TB_CUDA(cudaEventRecord(c->upload_ev[0], c->st));
   TB_CUDA(cudaStreamWaitEvent(c->copy_st, c->upload_ev[0], 0));
