@@ -158,7 +158,7 @@ typedef struct tribit_tuning {
   float count_ms;       /* tribit_autotune: measured counting time of this setting */
   float merge_ratio;    /* plain dispatch: a row block not sent to the tiles goes to the sorted-list
                            merge when its neighbours' bit rows average at least merge_ratio times
-                           its own rows' length, else to the bitmap sweep (default 2; 1e30 = never) */
+                           its own rows' length, else to the bitmap sweep (default 0.75; 1e30 = never) */
 } tribit_tuning;
 tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);
 /* Applies to later calls, and rebuilds the schedule of the prepared graph. */

@@ -1777,14 +1777,12 @@ __device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo
 
 // One pass over the edges of the merge row blocks. Modes 0 and 1: one warp
 // per row block; rows of at most kHubLaneRow neighbours are walked by their
-// own lane, longer rows by the whole warp. Mode 2: one warp per row, the
-// warps taking row blocks in increasing order from a device cursor (*cursor
-// starts at 0), so that the in-lists fill in (nearly) row order in one launch.
-// For the edge at CSR position j, u's tail is u's bit blocks from v's block
-// on. Mode 0: save[v] += the blocks a hub walk saves (v's row length - tail)
-// over the candidate edges. Mode 1: flags the edges whose hub saves at least
-// its staging cost and counts them per hub. Mode 2: appends each flagged
-// edge's tail (first block, length) and row to its hub's in-list.
+// own lane, longer rows by the whole warp. Mode 2: one warp per row. For the edge at CSR position j, u's tail is u's bit
+// blocks from v's block on. Mode 0: save[v] += the blocks a hub walk saves
+// (v's row length - tail) over the candidate edges. Mode 1: flags the edges
+// whose hub saves at least its staging cost and counts them per hub. Mode 2:
+// appends each flagged edge's tail (first block, length) and row to its hub's
+// in-list. rows (may be null): the pass covers rows [rows[0], rows[1]).
 constexpr uint32_t kHubLaneRow = 64;
 
 template <int Mode>
@@ -1792,10 +1790,11 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
                             unsigned long long* __restrict__ save, uint32_t* __restrict__ eflag,
                             uint32_t* __restrict__ in_cnt, const uint32_t* __restrict__ in_off,
                             uint64_t* __restrict__ inl, uint32_t* __restrict__ inrow,
-                            uint32_t* __restrict__ cursor) {
+                            const uint32_t* __restrict__ rows) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
   // Applies mode Mode to the edge at j (v = col[j], tail blocks) of row u.
   auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t v, uint32_t pos, uint32_t tail, bool hub,
                   uint32_t nbv) {
@@ -1838,25 +1837,20 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
     }
   };
   if constexpr (Mode == 2) {
-    const uint32_t nrb = (g.n + 31) >> 5;
-    for (;;) {
-      uint32_t rb = 0;
-      if (lane == 0) rb = atomicAdd(cursor, 1u);
-      rb = __shfl_sync(kFull, rb, 0);
-      if (rb >= nrb) break;
-      if (variant_of[rb] != TRIBIT_VARIANT_MERGE) continue;
-      for (uint32_t u = rb * 32; u < min(rb * 32 + 32, g.n); ++u) {
-        const uint64_t a = g.rp[u], b = g.rp[u + 1];
-        const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a);
-        if (re - rs >= 2) warp_row(u, rs, re, bs, rp_blk(b) - bs);
-      }
+    // The in-list fill runs once per row wave over few rows: one warp per row
+    // keeps every warp of the grid busy.
+    for (uint32_t u = u0 + warp; u < u1; u += nwarps) {
+      if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
+      const uint64_t a = g.rp[u], b = g.rp[u + 1];
+      const uint32_t rs = rp_row(a), re = rp_row(b), bs = rp_blk(a);
+      if (re - rs >= 2) warp_row(u, rs, re, bs, rp_blk(b) - bs);
     }
   } else {
-    for (uint32_t rb = warp; rb < ((g.n + 31) >> 5); rb += nwarps) {
+    for (uint32_t rb = (u0 >> 5) + warp; rb < ((u1 + 31) >> 5); rb += nwarps) {
       if (variant_of[rb] != TRIBIT_VARIANT_MERGE) continue;
       const uint32_t u = rb * 32 + lane;
       uint32_t rs = 0, re = 0, bs = 0, nbu = 0;
-      bool mine = u < g.n;
+      bool mine = u >= u0 && u < u1;
       if (mine) {
         const uint64_t a = g.rp[u], b = g.rp[u + 1];
         rs = rp_row(a);
@@ -2034,7 +2028,6 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.piece_wave = ar.take<uint8_t>(2 * n + E / kHubWarpPiece + 64);
     s.wave_lo = ar.take<uint32_t>(kHubWaves + 1);
     s.wave_cnt = ar.take<uint32_t>(2 * kHubWaves);
-    s.fill_cursor = ar.take<uint32_t>(1);
     s.hub_pos = ar.take<uint32_t>(2 * (n + 1));
     s.hub_scan_tmp = take_scan_temp<uint32_t>(ar, 2 * (n + 1));
   }
@@ -2066,11 +2059,11 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
   k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo);
   TB_LAUNCH_CHECK();
-  // In-lists filled in (nearly) row order, hence in wave order.
-  TB_CUDA(cudaMemsetAsync(s.fill_cursor, 0, sizeof(uint32_t), st));
-  k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow, s.fill_cursor);
-  TB_LAUNCH_CHECK();
+  for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
+    k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                             s.inrow, s.wave_lo + w);
+    TB_LAUNCH_CHECK();
+  }
   k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, s.vinfo, (uint32_t)n, s.hub_pos);
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.hub_pos, s.hub_pos, 2 * (n + 1), true, OpSum{}, 0u, s.hub_scan_tmp, st);

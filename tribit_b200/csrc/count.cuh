@@ -26,8 +26,11 @@ constexpr int kTileMaxK = 64;  // bit-tile variant: row blocks spanning at most 
 constexpr int kFeatSpan = 13;  // feature index of log2(1 + column-block span)
 constexpr uint32_t kMinPieceWidth = 32;  // piece_width is a multiple of 32, at least this
 // Plain dispatcher: a row block goes to the merge variant when its neighbours'
-// bit rows average at least this many times its own rows' length.
-constexpr float kDefaultMergeRatio = 2.f;
+// bit rows average at least this many times its own rows' length. Set once from
+// a sweep over RMAT-18..24, planted partition, Chung-Lu and Erdos-Renyi graphs:
+// 0.75 is within 2-6% of the per-graph best ratio on each of them (0.5 wins on
+// RMAT-22/24 but loses 48% on planted and Erdos-Renyi, 2.0 loses 96% on RMAT-24).
+constexpr float kDefaultMergeRatio = 0.75f;
 
 struct Schedule {
   uint32_t num_row_blocks = 0;
@@ -60,7 +63,6 @@ struct Schedule {
   uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail
   uint32_t* wave_lo = nullptr;     // device: first row of each wave, then n
   uint32_t* wave_cnt = nullptr;    // device: pieces per (list, wave), scanned to positions
-  uint32_t* fill_cursor = nullptr; // device: next row block of the in-list fill
   uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
   uint32_t* hub_scan_tmp = nullptr;
   bool hubs = true;                // build the hub lists for merge row blocks

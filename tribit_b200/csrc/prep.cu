@@ -380,49 +380,82 @@ __global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_
   }
 }
 
-// One warp per row: the row's distinct sorted values (front of its nbr slice)
-// to col, and its bit-row entries (block << 32 | mask) to bent, each written
-// once: the mask of a block is a segmented OR over the lanes holding its
-// values (a block cut by a chunk boundary carries its partial mask over).
+// The row's distinct sorted values (front of its nbr slice) to col, and its
+// bit-row entries (block << 32 | mask) to bent, each written once. One warp
+// per 32 rows: a row of at most kLaneEmit values is written by its own lane;
+// a longer one by the whole warp, where the mask of a block is a segmented OR
+// over the lanes holding its values (a block cut by a chunk boundary carries
+// its partial mask over). Most rows of a power-law graph hold 0 or 1 values.
+constexpr uint32_t kLaneEmit = 8;
 __global__ void k_emit_rows(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
                             const uint64_t* __restrict__ rp, uint32_t n, uint32_t* __restrict__ col,
                             uint64_t* __restrict__ bent) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t u = warp; u < n; u += nwarps) {
-    const uint64_t r0 = rp[u], r1 = rp[u + 1];
-    const uint32_t slot = (uint32_t)(r0 >> 32), nu = (uint32_t)(r1 >> 32) - slot, b0 = (uint32_t)r0;
-    const uint32_t* a = nbr + off[u];
-    // Blocks written so far; the previous chunk's last value and the partial
-    // mask of its last block.
-    uint32_t nblk = 0, last = kPad, carry = 0;
-    for (uint32_t c = 0; c < nu; c += 32) {
-      const uint32_t i = c + lane;
-      const bool in = i < nu;
-      const uint32_t x = in ? a[i] : kPad;
-      const uint32_t blk = x >> 5;
-      uint32_t prev = __shfl_up_sync(kFull, x, 1);
-      if (lane == 0) prev = last;
-      uint32_t next = __shfl_down_sync(kFull, x, 1);
-      if (lane == 31) next = c + 32 < nu ? a[c + 32] : kPad;
-      const bool new_blk = in && (i == 0 || blk != (prev >> 5));
-      const bool end_blk = in && (i + 1 == nu || blk != (next >> 5));
-      // Segmented OR of the block's bits from its first lane in this chunk.
-      uint32_t m = in ? 1u << (x & 31) : 0u;
-#pragma unroll
-      for (uint32_t o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(kFull, m, o);
-        const uint32_t yb = __shfl_up_sync(kFull, blk, o);
-        if (lane >= o && yb == blk) m |= y;
+  for (uint32_t ubase = warp * 32; ubase < n; ubase += nwarps * 32) {
+    const uint32_t mu = ubase + lane;
+    const bool here = mu < n;
+    uint32_t mslot = 0, mnu = 0, mb0 = 0, moff = 0;
+    if (here) {
+      const uint64_t r0 = rp[mu], r1 = rp[mu + 1];
+      mslot = (uint32_t)(r0 >> 32);
+      mnu = (uint32_t)(r1 >> 32) - mslot;
+      mb0 = (uint32_t)r0;
+      moff = mnu ? off[mu] : 0u;
+    }
+    if (here && mnu <= kLaneEmit && mnu > 0) {
+      const uint32_t* a = nbr + moff;
+      uint32_t nblk = 0, cur = a[0] >> 5, m = 0;
+      for (uint32_t i = 0; i < mnu; ++i) {
+        const uint32_t x = a[i];
+        col[mslot + i] = x;
+        if ((x >> 5) != cur) {
+          bent[mb0 + nblk++] = ((uint64_t)cur << 32) | m;
+          cur = x >> 5;
+          m = 0;
+        }
+        m |= 1u << (x & 31);
       }
-      if (i > 0 && c > 0 && blk == (last >> 5)) m |= carry;  // the block began in the previous chunk
-      const uint32_t incl = warp_inclusive_sum(new_blk ? 1u : 0u);
-      if (in) col[slot + i] = x;
-      if (end_blk) bent[b0 + nblk + incl - 1] = ((uint64_t)blk << 32) | m;
-      carry = __shfl_sync(kFull, m, 31);
-      last = __shfl_sync(kFull, x, 31);
-      nblk += __shfl_sync(kFull, incl, 31);
+      bent[mb0 + nblk] = ((uint64_t)cur << 32) | m;
+    }
+    uint32_t longer = __ballot_sync(kFull, here && mnu > kLaneEmit);
+    while (longer) {
+      const uint32_t r = __ffs(longer) - 1;
+      longer &= longer - 1;
+      const uint32_t slot = __shfl_sync(kFull, mslot, r), nu = __shfl_sync(kFull, mnu, r),
+                     b0 = __shfl_sync(kFull, mb0, r);
+      const uint32_t* a = nbr + __shfl_sync(kFull, moff, r);
+      // Blocks written so far; the previous chunk's last value and the partial
+      // mask of its last block.
+      uint32_t nblk = 0, last = kPad, carry = 0;
+      for (uint32_t c = 0; c < nu; c += 32) {
+        const uint32_t i = c + lane;
+        const bool in = i < nu;
+        const uint32_t x = in ? a[i] : kPad;
+        const uint32_t blk = x >> 5;
+        uint32_t prev = __shfl_up_sync(kFull, x, 1);
+        if (lane == 0) prev = last;
+        uint32_t next = __shfl_down_sync(kFull, x, 1);
+        if (lane == 31) next = c + 32 < nu ? a[c + 32] : kPad;
+        const bool new_blk = in && (i == 0 || blk != (prev >> 5));
+        const bool end_blk = in && (i + 1 == nu || blk != (next >> 5));
+        // Segmented OR of the block's bits from its first lane in this chunk.
+        uint32_t m = in ? 1u << (x & 31) : 0u;
+  #pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(kFull, m, o);
+          const uint32_t yb = __shfl_up_sync(kFull, blk, o);
+          if (lane >= o && yb == blk) m |= y;
+        }
+        if (i > 0 && c > 0 && blk == (last >> 5)) m |= carry;  // the block began in the previous chunk
+        const uint32_t incl = warp_inclusive_sum(new_blk ? 1u : 0u);
+        if (in) col[slot + i] = x;
+        if (end_blk) bent[b0 + nblk + incl - 1] = ((uint64_t)blk << 32) | m;
+        carry = __shfl_sync(kFull, m, 31);
+        last = __shfl_sync(kFull, x, 31);
+        nblk += __shfl_sync(kFull, incl, 31);
+      }
     }
   }
 }
