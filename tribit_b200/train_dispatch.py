@@ -58,7 +58,8 @@ def training_graphs(quick: bool):
         return [("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(4000, 103)), ("batch_s101", batch(64, 101)),
                 ("cliques_32x256", cliques(32, 256))]
     # RMAT at several scales: which variant wins a block shifts with the graph's size.
-    return [("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)), ("rmat20_s120", rmat(20, 120)),
+    return [("rmat23_s123", rmat(23, 123)), ("rmat22_s122", rmat(22, 122)), ("rmat21_s121", rmat(21, 121)),
+            ("rmat20_s120", rmat(20, 120)),
             ("rmat19_s119", rmat(19, 119)), ("rmat18_s118", rmat(18, 118)), ("planted_s103", planted(20000, 103)),
             ("batch_s101", batch(1024, 101)), ("cliques_96x384", cliques(96, 384))]
 
