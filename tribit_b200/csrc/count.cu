@@ -374,6 +374,14 @@ __device__ __forceinline__ unsigned long long cycles() { return (unsigned long l
 
 // ---- warp-per-piece kernels (bitmap and merge variants) --------------------
 
+// Merge row blocks' edges left to the row sweep (not taken by the hub pass)
+// are walked by sorted-list merge with binary searches (0), or, like the
+// bitmap variant's, as v's bit blocks probed in u's direct-mapped or hashed
+// row (1). Build-time switch for measurement.
+#ifndef TB_MERGE_BITS
+#define TB_MERGE_BITS 0
+#endif
+
 template <int V>
 __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, const uint64_t* __restrict__ pieces,
                                                                     const uint32_t* __restrict__ piece_off,
@@ -385,6 +393,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
   __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
   __shared__ uint32_t runs[kWarpsPerCta][64];
   __shared__ uint32_t s_row;
+  constexpr bool kSorted = V == TRIBIT_VARIANT_MERGE && !TB_MERGE_BITS;  // u staged as a sorted row
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* tbl = smem[w];
 
@@ -512,7 +521,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       if (u != cur) {
         __syncwarp();
         cur = u;
-        if (V == TRIBIT_VARIANT_MERGE) {
+        if (kSorted) {
           const uint32_t bs = rp_blk(a), be = rp_blk(b);
           d = be - bs;  // u's bit-row length
           cur_ok = d <= kWarpMaxBlocks;
@@ -551,7 +560,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       }
       const uint32_t cs = rs + first, ce = min(cs + width, re);
       uint64_t racc;
-      if (V == TRIBIT_VARIANT_MERGE) {
+      if (kSorted) {
         racc = sweep_merge(g, tbl, d, cs, ce);
       } else if (cur_direct) {
         const uint32_t span = bmax - bmin + 1;
@@ -1805,7 +1814,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
     } else if ((eflag[j >> 5] >> (j & 31)) & 1u) {
       const uint32_t at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
       inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
-      inrow[at] = u;
+      if (inrow) inrow[at] = u;  // timing mode only
     }
   };
   // Walks row u (CSR [rs, re), nb bit blocks from bs) with the whole warp.
@@ -1937,7 +1946,10 @@ __global__ void k_hub_total(const uint32_t* __restrict__ in_off, uint32_t n, uin
 // time, so each hub's in-list is ordered by wave, and the hub pieces are then
 // ordered by the wave of their first tail: the CTAs working at one time walk
 // the tails of rows of one wave, whose bit rows fit the L2.
-__global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo) {
+// wave_bk[w] = the bit-row start of wave w's first row: the wave of row u is
+// the last w with wave_bk[w] <= k for any bit-row index k of u's row (a tail
+// start), so a piece's wave follows from its first tail without its row.
+__global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo, uint32_t* __restrict__ wave_bk) {
   const uint32_t w = threadIdx.x;
   if (w > kHubWaves) return;
   const uint64_t nb = rp_blk(g.rp[g.n]);
@@ -1951,26 +1963,27 @@ __global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo) {
       hi = mid;
   }
   wave_lo[w] = w == kHubWaves ? g.n : lo;
+  wave_bk[w] = w == kHubWaves ? 0xFFFFFFFFu : rp_blk(g.rp[lo]);
 }
 
-__device__ __forceinline__ uint32_t wave_of(const uint32_t* __restrict__ wave_lo, uint32_t u) {
+__device__ __forceinline__ uint32_t wave_of_block(const uint32_t* __restrict__ wave_bk, uint32_t k) {
   uint32_t w = 0;
 #pragma unroll
   for (uint32_t st = kHubWaves / 2; st >= 1; st >>= 1)
-    if (w + st < kHubWaves && wave_lo[w + st] <= u) w += st;
+    if (w + st < kHubWaves && wave_bk[w + st] <= k) w += st;
   return w;
 }
 
 // Counting sort of the hub pieces by the wave of their first tail, within
 // each list (CTA pieces [0, Pc), warp pieces [Pc, P)). cnt: 2 kHubWaves.
 __global__ void k_piece_waves(const uint64_t* __restrict__ pieces, const uint32_t* __restrict__ piece_off,
-                              const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ inrow,
-                              const uint32_t* __restrict__ wave_lo, uint32_t* __restrict__ cnt,
+                              const uint32_t* __restrict__ in_off, const uint64_t* __restrict__ inl,
+                              const uint32_t* __restrict__ wave_bk, uint32_t* __restrict__ cnt,
                               uint8_t* __restrict__ wave) {
   const uint32_t pc_n = piece_off[TRIBIT_NUM_VARIANTS + 2], all = piece_off[TRIBIT_NUM_VARIANTS + 3];
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < all; p += gridDim.x * blockDim.x) {
     const uint64_t pc = pieces[p];
-    const uint32_t w = wave_of(wave_lo, inrow[in_off[pc >> 32] + (uint32_t)pc]);
+    const uint32_t w = wave_of_block(wave_bk, (uint32_t)(inl[in_off[pc >> 32] + (uint32_t)pc] >> 32));
     wave[p] = (uint8_t)w;
     atomicAdd(&cnt[(p < pc_n ? 0 : kHubWaves) + w], 1u);
   }
@@ -2027,6 +2040,7 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.hub_pieces2 = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
     s.piece_wave = ar.take<uint8_t>(2 * n + E / kHubWarpPiece + 64);
     s.wave_lo = ar.take<uint32_t>(kHubWaves + 1);
+    s.wave_bk = ar.take<uint32_t>(kHubWaves + 1);
     s.wave_cnt = ar.take<uint32_t>(2 * kHubWaves);
     s.hub_pos = ar.take<uint32_t>(2 * (n + 1));
     s.hub_scan_tmp = take_scan_temp<uint32_t>(ar, 2 * (n + 1));
@@ -2057,11 +2071,11 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.in_cnt, s.in_off, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
-  k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo);
+  k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo, s.wave_bk);
   TB_LAUNCH_CHECK();
   for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
     k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                             s.inrow, s.wave_lo + w);
+                                             s.hub_rows ? s.inrow : nullptr, s.wave_lo + w);
     TB_LAUNCH_CHECK();
   }
   k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, s.vinfo, (uint32_t)n, s.hub_pos);
@@ -2072,7 +2086,7 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   k_hub_total<<<1, 1, 0, st>>>(s.in_off, (uint32_t)n, s.piece_off);
   TB_LAUNCH_CHECK();
   TB_CUDA(cudaMemsetAsync(s.wave_cnt, 0, 2 * kHubWaves * sizeof(uint32_t), st));
-  k_piece_waves<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.in_off, s.inrow, s.wave_lo, s.wave_cnt,
+  k_piece_waves<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.in_off, s.inl, s.wave_bk, s.wave_cnt,
                                           s.piece_wave);
   TB_LAUNCH_CHECK();
   k_wave_scan<<<1, 1, 0, st>>>(s.wave_cnt, s.piece_off);

@@ -62,11 +62,13 @@ struct Schedule {
   uint64_t* hub_pieces2 = nullptr; // device: the pieces in hub order, before the wave sort
   uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail
   uint32_t* wave_lo = nullptr;     // device: first row of each wave, then n
+  uint32_t* wave_bk = nullptr;     // device: bit-row start of each wave's first row
   uint32_t* wave_cnt = nullptr;    // device: pieces per (list, wave), scanned to positions
   uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
   uint32_t* hub_scan_tmp = nullptr;
   bool hubs = true;                // build the hub lists for merge row blocks
   bool hubs_active = false;        // set by build_pieces
+  bool hub_rows = false;           // also write each in-list entry's row (read by the timing mode only)
   uint32_t piece_width = 64;       // neighbours per piece (tuned)
   float tile_min_nnz = 64.f;       // plain dispatcher: fewest edges for a bit-tile row block (tuned)
   float merge_ratio = kDefaultMergeRatio;  // plain dispatcher: merge where neighbours' bit rows are this much longer

@@ -521,7 +521,9 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     TB_CUDA(cudaMemsetAsync(ns, 0, (nrb + 1) * sizeof(unsigned long long), c->st));
     if (nrb) TB_CUDA(cudaMemsetAsync(c->sched.variant_of, variant, nrb, c->st));
     c->sched.hubs = variant == TRIBIT_VARIANT_MERGE;
+    c->sched.hub_rows = true;  // the hub pieces charge their cycles to their rows' blocks
     tb::build_pieces(c->prep.view, c->sched, c->st);
+    c->sched.hub_rows = false;
     tb::CountConfig cfg = tb::count_config(c);
     cfg.block_ns = ns;
     cfg.variant_start = c->ev[0];
