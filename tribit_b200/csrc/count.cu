@@ -1212,7 +1212,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 
 // Build-time tunables (-D...): measured defaults.
 #ifndef TB_HUB_PIECE
-#define TB_HUB_PIECE 1024
+#define TB_HUB_PIECE 512
 #endif
 #ifndef TB_HUB_DEPTH
 #define TB_HUB_DEPTH 4
@@ -1240,7 +1240,7 @@ constexpr uint32_t kHubHashMin = TB_HUB_HASH_MIN;  // ... plus this many blocks 
 constexpr uint32_t kHubWarpHash = kHubWarpSpan / 4;        // bit blocks: warp hash
 constexpr uint32_t kHubPiece = TB_HUB_PIECE;    // in-edges per CTA piece
 #ifndef TB_HUB_WARP_PIECE
-#define TB_HUB_WARP_PIECE 256
+#define TB_HUB_WARP_PIECE 128
 #endif
 constexpr uint32_t kHubWarpPiece = TB_HUB_WARP_PIECE;  // in-edges per warp piece
 #ifndef TB_HUB_WAVES
