@@ -242,7 +242,10 @@ tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, c
  * reserves 95% of free memory at start-up), or a latency-bound loop that must
  * not pay the implicit synchronisation of cudaMalloc / cudaFree.
  * Counts the graph in d_entries (device memory, zipped words as for
- * tribit_count_edges; degree order, plain dispatch) on `stream` (a
+ * tribit_count_edges; degree order; bit tiles or the bitmap sweep, without the
+ * merge variant's hub lists, which do not fit the scratch: on power-law graphs
+ * the counting kernels then run 2-3 times longer than a context's learned
+ * dispatch) on `stream` (a
  * cudaStream_t; NULL = the legacy default stream), taking every intermediate
  * buffer from one fixed scratch array compiled into the library
  * (tribit_noalloc_scratch_bytes() = 32 MiB, held on each device that loads it

@@ -1218,7 +1218,10 @@ __global__ void __launch_bounds__(kCtaThreads) k_rows_global(GraphView g, const 
 #define TB_HUB_DEPTH 4
 #endif
 constexpr int kHubWarps = 8;
-constexpr uint32_t kHubMaxSpan = 8192;          // blocks of v's row span: 32 KiB of masks
+#ifndef TB_HUB_MAX_SPAN
+#define TB_HUB_MAX_SPAN 8192
+#endif
+constexpr uint32_t kHubMaxSpan = TB_HUB_MAX_SPAN;  // blocks of v's row span staged direct-mapped by a CTA (4 bytes each)
 constexpr uint32_t kHubWarpSpan = kHubMaxSpan / kHubWarps;  // spans up to this: one warp per piece
 // A warp's slice of the map: its span plus a zero word past the staged masks,
 // rounded to 16 bytes for the hash buckets (16-byte loads).
@@ -1247,7 +1250,12 @@ constexpr uint32_t kHubWarpPiece = TB_HUB_WARP_PIECE;  // in-edges per warp piec
 #define TB_HUB_WAVES 32
 #endif
 constexpr uint32_t kHubWaves = TB_HUB_WAVES;    // row ranges the hub pieces are ordered by (power of 2)
-constexpr int kHubCtasPerSm = 5;
+// Five CTAs per SM (48 registers), the occupancy the 41 KiB of shared memory
+// allows; with four the pair loads' extra registers cost more than they save.
+#ifndef TB_HUB_MIN_CTAS
+#define TB_HUB_MIN_CTAS 5
+#endif
+constexpr int kHubCtasPerSm = TB_HUB_MIN_CTAS;
 constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lane
 #ifndef TB_HUB_PAIRS
 #define TB_HUB_PAIRS 1
@@ -1368,11 +1376,6 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
 }
 
-// Five CTAs per SM (48 registers), the occupancy the 41 KiB of shared memory
-// allows; with four the pair loads' extra registers cost more than they save.
-#ifndef TB_HUB_MIN_CTAS
-#define TB_HUB_MIN_CTAS 5
-#endif
 __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
                                                         const uint32_t* __restrict__ in_off,
