@@ -27,3 +27,19 @@ def test_peak_is_the_measured_copy_bandwidth_when_present():
         assert (peak, kind) == (json.load(open(path))["hbm_gbs"], "measured")
     else:
         assert kind == "fallback" and peak > 0
+
+
+def test_reference_arm_graph_loads_no_product_code():
+    # The reference arm builds its R-MAT graph with the oracle's generator, so
+    # neither the product package nor its library is loaded by it.
+    import subprocess
+    import sys
+    code = ("import sys, json; sys.path.insert(0, %r); import bench; "
+            "n, e = bench.reference_graph({'gen': 'rmat', 'scale': 12, 'edge_factor': 16, 'seed': 12}); "
+            "print(json.dumps([n, int(e.size), 'tribit_b200' in sys.modules, "
+            "any('libtribit' in l for l in open('/proc/self/maps'))]))") % ROOT
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    import json
+    n, size, imported, mapped = json.loads(out.stdout.strip().splitlines()[-1])
+    assert (n, size) == (1 << 12, 16 << 12) and not imported and not mapped
