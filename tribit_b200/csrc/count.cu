@@ -1848,9 +1848,10 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
       if (in) edge(u, bs, j, v, pos, tail, hub, nbv);
     }
   };
-  if constexpr (Mode == 2) {
-    // The in-list fill runs once per row wave over few rows: one warp per row
-    // keeps every warp of the grid busy.
+  if (Mode == 2 && u1 - u0 < 32u * nwarps) {
+    // The in-list fill runs once per row wave; a wave of fewer rows than the
+    // grid has lanes keeps every warp busy with one warp per row. Larger waves
+    // (the first ones: millions of short rows) take the row-block loop below.
     for (uint32_t u = u0 + warp; u < u1; u += nwarps) {
       if (variant_of[u >> 5] != TRIBIT_VARIANT_MERGE) continue;
       const uint64_t a = g.rp[u], b = g.rp[u + 1];
@@ -1882,7 +1883,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           }
           const uint32_t tail = nbu - pos;
           uint32_t nbv = 0;
-          const bool hub = hub_candidate<Mode>(vinfo, save, v, tail, nbv);
+          const bool hub = Mode != 2 && hub_candidate<Mode>(vinfo, save, v, tail, nbv);
           if (Mode == 1 && hub) atomicOr(&eflag[j >> 5], 1u << (j & 31));
           edge(u, bs, j, v, pos, tail, hub, nbv);
         }

@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_
     for (uint32_t k = 2; k <= P; k <<= 1) {
       for (uint32_t j = k >> 1; j > 0; j >>= 1) {
         for (uint32_t t = tid; t < P / 2; t += blockDim.x) {
-          const uint32_t i = 2 * j * (t / j) + (t % j);  // pairs (i, i + j)
+          const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));  // pairs (i, i + j); j is a power of 2
           const bool up = (i & k) == 0;
           const uint32_t x = a[i], y = a[i + j];
           if (up ? x > y : x < y) {
