@@ -48,13 +48,22 @@ __device__ __forceinline__ bool load_entry(const PrepInput& in, uint64_t i, uint
   return a != b;
 }
 
-// Degrees (with duplicates) over entries [i0, i1).
+// The degree order only has to be a good order (any total order counts every
+// triangle once): degrees may be counted over every kDegreeSample-th entry
+// (a strided sample, which a sorted input does not bias). Every entry is still
+// checked for range when it is oriented (k_row_count).
+#ifndef TB_DEGREE_SAMPLE
+#define TB_DEGREE_SAMPLE 1
+#endif
+constexpr uint64_t kDegreeSample = TB_DEGREE_SAMPLE;
+
+// Degrees (with duplicates) over the sampled entries of [i0, i1).
 __global__ void k_degree(PrepInput in, uint64_t i0, uint64_t i1, uint32_t* __restrict__ deg, unsigned int* err) {
-  uint64_t i = i0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (; i < i1; i += stride) {
+  const uint64_t first = (i0 + kDegreeSample - 1) / kDegreeSample, last = (i1 + kDegreeSample - 1) / kDegreeSample;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t s = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < last; s += stride) {
     uint32_t a, b;
-    if (load_entry(in, i, a, b, err)) {
+    if (load_entry(in, s * kDegreeSample, a, b, err)) {
       atomicAdd(&deg[a], 1u);
       atomicAdd(&deg[b], 1u);
     }
