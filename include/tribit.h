@@ -102,8 +102,17 @@ typedef struct tribit_result {
   uint32_t load_gpu_parse;    /* 1 when the GPU parsed the file, 0 when the host grammar did */
   uint32_t stream_ranges;     /* tribit_count_edges: 1 when the graph fit the device budget, else the
                                  rank ranges it was counted in (see tribit_set_device_budget) */
-  uint32_t stream_tasks;      /* counts of range pairs those ranges took (1 in one piece) */
+  uint32_t stream_tasks;      /* device counts those ranges took: 1 in one piece and with
+                                 TRIBIT_STREAM_ROWS, one per pair of ranges with TRIBIT_STREAM_PAIRS */
+  uint32_t stream_tier;       /* 0 (one piece), TRIBIT_STREAM_ROWS or TRIBIT_STREAM_PAIRS */
 } tribit_result;
+
+/* How tribit_count_edges counts a graph past the device budget. */
+enum {
+  TRIBIT_STREAM_AUTO = 0,  /* ROWS when the oriented rows fit the budget, else PAIRS */
+  TRIBIT_STREAM_ROWS = 1,  /* rows built one rank range at a time, kept on the device, counted once */
+  TRIBIT_STREAM_PAIRS = 2  /* each pair of rank ranges counted as a graph of its own */
+};
 
 typedef struct tribit_context tribit_context;
 
@@ -125,11 +134,16 @@ const char* tribit_version(void);
  * A graph whose device buffers exceed the context's device budget (all the
  * memory the device has free, unless tribit_set_device_budget says less) is
  * counted in pieces: its entries are streamed through the GPU to rank them
- * and sort them into host buckets by rank range, and each pair of ranges is
- * then counted on the device (result.stream_ranges > 1). The reference splits
- * a graph too large for a GPU into partitions and tasks of at most 1e9
- * entries over several GPUs (src/multi_gpu/src/main.rs:98-220). Such a count
- * leaves no prepared graph in the context (tribit_launch_count then fails). */
+ * and sort them into host buckets by rank range (result.stream_ranges > 1).
+ * Then either each range's rows are built on the device in turn into one
+ * oriented graph that stays resident and is counted once (TRIBIT_STREAM_ROWS:
+ * the preprocessing scratch is what did not fit), or, when even the rows do
+ * not fit, each pair of ranges is counted on the device as a graph of its own
+ * (TRIBIT_STREAM_PAIRS). The reference splits a graph too large for a GPU into
+ * partitions and tasks of at most 1e9 entries over several GPUs
+ * (src/multi_gpu/src/main.rs:98-220). A TRIBIT_STREAM_ROWS count leaves the
+ * graph prepared for tribit_launch_count; a TRIBIT_STREAM_PAIRS count leaves
+ * none (tribit_launch_count then fails). */
 tribit_status tribit_count_edges(tribit_context* ctx, const uint64_t* entries, uint64_t n_entries, uint64_t num_nodes,
                                  tribit_result* out);
 /* Device memory (bytes) a one-piece tribit_count_edges of n_entries entries on
@@ -138,6 +152,12 @@ tribit_status tribit_device_bytes(tribit_context* ctx, uint64_t n_entries, uint6
 /* Caps the device memory later tribit_count_edges calls of this context may
  * use (bytes; 0 = what the device has free at the call). */
 tribit_status tribit_set_device_budget(tribit_context* ctx, uint64_t bytes);
+/* Streamed counts of later tribit_count_edges calls: `tier` one of
+ * TRIBIT_STREAM_*, `range_entries` an upper bound on the oriented entries of a
+ * rank range (0: as many as the budget allows; a bound at or below the
+ * longest row fails with TRIBIT_ERR_OUT_OF_MEMORY). A forced tier that cannot
+ * fit the budget fails with TRIBIT_ERR_OUT_OF_MEMORY. */
+tribit_status tribit_set_stream_options(tribit_context* ctx, int tier, uint64_t range_entries);
 /* Same with the entries already in device memory. */
 tribit_status tribit_count_edges_device(tribit_context* ctx, const uint64_t* d_entries, uint64_t n_entries,
                                         uint64_t num_nodes, tribit_result* out);

@@ -48,6 +48,8 @@ def test_invalid_arguments():
     assert tb.lib.tribit_count_edges(None, None, 0, 0, None) == 1
     assert tb.lib.tribit_launch_count(None) == 1
     assert tb.lib.tribit_set_stream(None, None) == 1
+    assert tb.lib.tribit_set_stream_options(None, 0, 0) == 1
+    assert tb.lib.tribit_set_device_budget(None, 0) == 1
 
 
 def test_generators_deterministic():

@@ -37,6 +37,7 @@ lib = ctypes.CDLL(LIB_PATH)
 
 ORDERS = {"degree": 0, "id": 1}
 DISPATCH = {"plain": 0, "learned": 1, "merge": 2, "bitmap": 3, "mma": 4}
+STREAM_TIERS = {"auto": 0, "rows": 1, "pairs": 2}
 VARIANTS = ("mma", "bitmap", "merge")
 TILE_ENGINES = ("mma_sync", "tcgen05")
 
@@ -56,7 +57,7 @@ class _Result(ctypes.Structure):
                 ("h2d_ms", ctypes.c_float), ("preprocess_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("count_kernels", _u32), ("hub_edges", _u32),
                 ("load_ms", ctypes.c_float), ("load_gpu_parse", _u32), ("stream_ranges", _u32),
-                ("stream_tasks", _u32)]
+                ("stream_tasks", _u32), ("stream_tier", _u32)]
 
 
 def _decl(name, res, *args):
@@ -75,6 +76,7 @@ _decl("tribit_last_error", ctypes.c_char_p, _p)
 _decl("tribit_version", ctypes.c_char_p)
 _decl("tribit_count_edges", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
 _decl("tribit_set_device_budget", ctypes.c_int, _p, _u64)
+_decl("tribit_set_stream_options", ctypes.c_int, _p, ctypes.c_int, _u64)
 _decl("tribit_device_bytes", ctypes.c_int, _p, _u64, _u64, ctypes.POINTER(_u64))
 _decl("tribit_count_edges_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
 _decl("tribit_prepare_device", ctypes.c_int, _p, _p, _u64, _u64, ctypes.POINTER(_Result))
@@ -165,12 +167,14 @@ class Result:
     load_gpu_parse: int = 0
     stream_ranges: int = 0
     stream_tasks: int = 0
+    stream_tier: int = 0
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         return cls(r.triangles, r.num_nodes, r.entries, r.edges, r.blocks_of_threads, r.row_blocks,
                    tuple(r.row_blocks_by_variant), r.h2d_ms, r.preprocess_ms, r.kernel_ms, r.total_ms,
-                   r.count_kernels, r.hub_edges, r.load_ms, r.load_gpu_parse, r.stream_ranges, r.stream_tasks)
+                   r.count_kernels, r.hub_edges, r.load_ms, r.load_gpu_parse, r.stream_ranges, r.stream_tasks,
+                   r.stream_tier)
 
 
 def _entries(a) -> np.ndarray:
@@ -327,6 +331,13 @@ class Counter:
         """Device memory later count_edges calls may use (0 = what is free); a
         graph needing more is counted in rank ranges (Result.stream_ranges > 1)."""
         _check(lib.tribit_set_device_budget(self._h, int(nbytes)), self._h)
+
+    def set_stream_options(self, tier: str = "auto", range_entries: int = 0):
+        """How a count past the device budget runs: "rows" builds the oriented
+        rows one rank range at a time and counts them once, "pairs" counts each
+        pair of ranges as its own graph, "auto" takes rows when they fit.
+        range_entries bounds a range's oriented entries (0: the budget's)."""
+        _check(lib.tribit_set_stream_options(self._h, STREAM_TIERS[tier], int(range_entries)), self._h)
 
     def device_bytes(self, n_entries: int, num_nodes: int) -> int:
         """Device memory a one-piece count_edges of this size takes."""

@@ -30,13 +30,20 @@ class Arena {
   size_t used() const { return off_; }
   size_t capacity() const { return cap_; }
 
-  void reserve(size_t bytes) {
+  // headroom: 1/16 more, so that slightly larger calls reuse the allocation
+  // (taken only when it can be had; never under a device budget).
+  void reserve(size_t bytes, bool headroom = true) {
     if (bytes <= cap_) return;
     if (base_ && !owned_)
       throw StatusError(TRIBIT_ERR_TOO_LARGE, "graph needs more scratch than the fixed device buffer holds");
     release();
-    size_t want = bytes + (bytes >> 4);  // headroom so slightly larger calls reuse it
+    size_t want = headroom ? bytes + (bytes >> 4) : bytes;
     cudaError_t e = cudaMalloc(&base_, want);
+    if (e != cudaSuccess && want != bytes) {
+      (void)cudaGetLastError();
+      want = bytes;
+      e = cudaMalloc(&base_, want);
+    }
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
       base_ = nullptr;
@@ -56,6 +63,14 @@ class Arena {
   }
 
   bool measuring() const { return measuring_; }
+
+  // Moves the layout cursor back to `at` (a used() of this pass): later takes
+  // reuse the space after it, which the caller no longer needs once the work
+  // queued on it has run (stream order).
+  void rewind(size_t at) {
+    if (at > off_) throw StatusError(TRIBIT_ERR_INTERNAL, "arena rewound past its cursor");
+    off_ = at;
+  }
 
   void release() {
     if (base_ && owned_) cudaFree(base_);

@@ -60,7 +60,7 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
   const bool stage = host_entries != nullptr;
   CallLayout L;
   layout(c, true, in, stage, G, &L);
-  c->arena.reserve(c->arena.used());
+  c->arena.reserve(c->arena.used(), c->device_budget == 0);
   layout(c, false, in, stage, G, &L);
   cudaStream_t st = c->st;
   TB_CUDA(cudaEventRecord(c->ev[0], st));
@@ -144,10 +144,6 @@ void count_device_input(tribit_context* c, const uint64_t* d_entries, uint64_t E
   run_call(c, in, nullptr, nullptr, nullptr, 0, true, res);
 }
 
-}  // namespace tb
-
-namespace {
-
 void fill_schedule_stats(tribit_context* c, tribit_result* res) {
   uint32_t lens[TRIBIT_NUM_VARIANTS], hub_edges = 0;
   TB_CUDA(cudaMemcpyAsync(lens, c->sched.list_len, sizeof lens, cudaMemcpyDeviceToHost, c->st));
@@ -162,7 +158,9 @@ void fill_schedule_stats(tribit_context* c, tribit_result* res) {
   }
 }
 
-}  // namespace
+}  // namespace tb
+
+using tb::fill_schedule_stats;
 
 extern "C" {
 
@@ -286,6 +284,7 @@ tribit_status tribit_count_edges(tribit_context* c, const uint64_t* entries, uin
       fill_schedule_stats(c, out);
       out->stream_ranges = 1;
       out->stream_tasks = 1;
+      out->stream_tier = 0;
     }
   });
 }

@@ -98,6 +98,7 @@ enum : uint32_t {
   kErrIdRange = 1u << 0,    // an entry named a vertex >= num_nodes
   kErrReserved = 1u << 1,   // never set (kept so the flag values stay those of the C-ABI)
   kErrTimeout = 1u << 2,    // a bounded wait gave up
+  kErrInput = 1u << 3,      // streamed counts: host entries changed between their passes
 };
 
 }  // namespace tb

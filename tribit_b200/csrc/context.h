@@ -52,6 +52,8 @@ struct tribit_context {
   // Device memory the context may use (tribit_set_device_budget; 0: what the
   // device has free); graphs needing more are counted in rank ranges.
   uint64_t device_budget = 0;
+  int stream_tier = 0;                 // TRIBIT_STREAM_* (tribit_set_stream_options)
+  uint64_t stream_range_entries = 0;   // bound on a rank range's entries (0: the budget's)
   tb::Arena stream_arena;              // streamed counts: degrees, ranks, row counts, piece buffers
   tb::Arena train_arena;               // training batches and activations
   tb::Arena timing_arena;              // per-row-block cycle counters
@@ -104,6 +106,9 @@ size_t call_bytes(tribit_context* c, uint64_t E, uint64_t n, int order, bool sta
 // dispatcher (tribit_count_edges_device with an explicit order).
 void count_device_input(tribit_context* c, const uint64_t* d_entries, uint64_t E, uint64_t n, int order,
                         tribit_result* res);
+// result.row_blocks, row_blocks_by_variant and hub_edges of the schedule in
+// the context (synchronises its stream).
+void fill_schedule_stats(tribit_context* c, tribit_result* res);
 // Counts host entries in rank ranges when their buffers exceed the device
 // budget (stream.cu). Returns false, doing nothing, when they fit.
 bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t E, uint64_t n, tribit_result* res);

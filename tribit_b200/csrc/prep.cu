@@ -475,6 +475,44 @@ __global__ void k_finalize(const uint64_t* __restrict__ rp, uint64_t n, DeviceSt
   stats->blocks = tot & 0xffffffffull;
 }
 
+// Range-relative row starts of rows [s, s + z]: off[k] = cursor[k] =
+// row_start[s + k] - row_start[s].
+__global__ void k_range_starts(const uint64_t* __restrict__ row_start, uint32_t s, uint32_t z,
+                               uint32_t* __restrict__ off, uint32_t* __restrict__ cursor) {
+  const uint64_t base = row_start[s];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= z; k += gridDim.x * blockDim.x) {
+    const uint32_t v = (uint32_t)(row_start[s + k] - base);
+    off[k] = v;
+    cursor[k] = v;
+  }
+}
+
+// The range's keys into their rows' slots (any order within a row).
+__global__ void k_range_fill(const uint64_t* __restrict__ keys, uint64_t cnt, uint32_t s, uint32_t z,
+                             const uint32_t* __restrict__ off, uint32_t* __restrict__ cursor,
+                             uint32_t* __restrict__ nbr, unsigned int* err) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t key = keys[i];
+    const uint32_t r = (uint32_t)(key >> 32) - s;
+    if (r >= z) {
+      atomicOr(err, kErrInput);
+      continue;
+    }
+    const uint32_t pos = atomicAdd(&cursor[r], 1u);
+    if (pos >= off[r + 1]) {
+      atomicOr(err, kErrInput);
+      continue;
+    }
+    nbr[pos] = (uint32_t)key;
+  }
+}
+
+// rp[k] += *carry, k < count: the range's prefix continues the ranges before.
+__global__ void k_range_carry(uint64_t* __restrict__ rp, uint32_t count, const uint64_t* __restrict__ carry) {
+  const uint64_t c = *carry;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) rp[k] += c;
+}
+
 void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t st, Prepared* out,
               DeviceStats* stats, uint64_t* rp) {
   const uint64_t E = in.E, n = in.n;
@@ -533,6 +571,55 @@ void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t
 }
 
 }  // namespace
+
+RowRangeBuffers take_row_range_buffers(Arena& ar, uint64_t n, uint64_t cap) {
+  RowRangeBuffers b;
+  b.keys = ar.take<uint64_t>(cap + 1);
+  b.scratch = reinterpret_cast<uint32_t*>(b.keys);
+  b.nbr = ar.take<uint32_t>(cap ? cap : 1);
+  b.off = ar.take<uint32_t>(n + 1);
+  b.cursor = ar.take<uint32_t>(n + 1);
+  b.big = ar.take<uint32_t>(n + 1);
+  b.nbig = ar.take<uint32_t>(1);
+  b.carry = ar.take<uint64_t>(1);
+  b.scan_tmp = take_scan_temp<uint64_t>(ar, n + 1);
+  return b;
+}
+
+void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t cnt,
+                     uint64_t* rp, uint32_t* col, uint64_t* bent, unsigned int* err, cudaStream_t st) {
+  if (z == 0) return;
+  // The ranges before this one left rp[s] = the prefix at row s, which the
+  // row sort below overwrites.
+  if (s == 0)
+    TB_CUDA(cudaMemsetAsync(b.carry, 0, sizeof(uint64_t), st));
+  else
+    TB_CUDA(cudaMemcpyAsync(b.carry, rp + s, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  TB_CUDA(cudaMemsetAsync(b.nbig, 0, sizeof(uint32_t), st));
+  k_range_starts<<<grid_for((uint64_t)z + 1), kThreads, 0, st>>>(row_start, s, z, b.off, b.cursor);
+  TB_LAUNCH_CHECK();
+  if (cnt > 0) {
+    k_range_fill<<<grid_for(cnt, 8), kThreads, 0, st>>>(b.keys, cnt, s, z, b.off, b.cursor, b.nbr, err);
+    TB_LAUNCH_CHECK();
+  }
+  const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(z, 8), 148ull * 32));
+  k_sort_rows<<<wgrid, kThreads, 0, st>>>(b.off, z, b.nbr, rp + s, b.big, b.nbig);
+  TB_LAUNCH_CHECK();
+  if (cnt > kWarpSortMax) {
+    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(b.off, b.nbr, b.scratch, rp + s, b.big, b.nbig);
+    TB_LAUNCH_CHECK();
+  }
+  device_scan<uint64_t, OpSum>(rp + s, rp + s, (uint64_t)z + 1, true, OpSum{}, 0ull, b.scan_tmp, st);
+  k_range_carry<<<grid_for((uint64_t)z + 1), kThreads, 0, st>>>(rp + s, z + 1, b.carry);
+  TB_LAUNCH_CHECK();
+  k_emit_rows<<<wgrid, kThreads, 0, st>>>(b.off, b.nbr, rp + s, z, col, bent);
+  TB_LAUNCH_CHECK();
+}
+
+void finalize_rows(const uint64_t* rp, uint64_t n, DeviceStats* stats, cudaStream_t st) {
+  k_finalize<<<1, 1, 0, st>>>(rp, n, stats);
+  TB_LAUNCH_CHECK();
+}
 
 RankBuffers take_rank_buffers(Arena& ar, uint64_t n) {
   RankBuffers b;

@@ -93,4 +93,31 @@ struct RankBuffers {
 RankBuffers take_rank_buffers(Arena& ar, uint64_t n);
 void rank_vertices(const uint32_t* deg, uint64_t n, uint64_t E, const RankBuffers& b, uint32_t* rank, cudaStream_t st);
 
+// One rank range's rows at a time: the oriented graph's rows [s, s + z) built
+// from that range's keys alone (lo << 32 | hi in rank space, lo in the range,
+// duplicates allowed), with the row sorts and the CSR / bit-row emission of
+// preprocessing, into the same rp / col / bent a one-piece build gives. Built
+// in increasing s, the ranges leave rp, col and bent equal to the one-piece
+// arrays, with scratch for one range (at most `cap` keys) instead of the graph.
+struct RowRangeBuffers {
+  uint64_t* keys = nullptr;     // cap + 1 words: the range's keys (the caller fills them)
+  uint32_t* scratch = nullptr;  // the same memory: long rows' sort space after the fill
+  uint32_t* nbr = nullptr;      // cap: the range's rows
+  uint32_t* off = nullptr;      // n + 1: range-relative row starts
+  uint32_t* cursor = nullptr;   // n + 1: fill cursors
+  uint32_t* big = nullptr;      // n + 1: rows for the CTA sort
+  uint32_t* nbig = nullptr;
+  uint64_t* carry = nullptr;    // rp of the range's first row before the range is built
+  uint64_t* scan_tmp = nullptr;
+};
+RowRangeBuffers take_row_range_buffers(Arena& ar, uint64_t n, uint64_t cap);
+// row_start: n + 1 exclusive prefix of the rows' key counts (duplicates
+// included); cnt = row_start[s + z] - row_start[s] keys in b.keys. A key whose
+// row or slot is out of place (the entries changed between the passes that
+// counted and bucketed them) is dropped and sets kErrInput in *err.
+void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t cnt,
+                     uint64_t* rp, uint32_t* col, uint64_t* bent, unsigned int* err, cudaStream_t st);
+// Edge and bit-block totals of rp[n] into stats.
+void finalize_rows(const uint64_t* rp, uint64_t n, DeviceStats* stats, cudaStream_t st);
+
 }  // namespace tb

@@ -258,6 +258,135 @@ void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* d
   TB_CUDA(cudaStreamWaitEvent(c->st, c->upload_ev[3], 0));
 }
 
+namespace {
+
+// The rows tier's device layout: the oriented graph's rows and the row starts
+// (kept), one range's build buffers, and over those buffers (dead once the
+// rows are built) the counting schedule. Returns the arena bytes.
+struct RowsLayout {
+  DeviceStats* stats = nullptr;
+  uint64_t* rp = nullptr;
+  uint32_t* col = nullptr;
+  uint64_t* bent = nullptr;
+  uint64_t* row_start = nullptr;
+  RowRangeBuffers build;
+  Schedule sched;
+};
+
+size_t rows_layout(Arena& ar, bool measure, uint64_t n, uint64_t kept, uint64_t cap, bool hubs, RowsLayout* L) {
+  ar.begin(measure);
+  L->stats = ar.take<DeviceStats>(1);
+  L->rp = ar.take<uint64_t>(n + 1);
+  L->col = ar.take<uint32_t>(kept ? kept : 1);
+  L->bent = ar.take<uint64_t>(kept + 2);  // + 2: 16-byte pair loads may read one entry past the end
+  const size_t rows_end = ar.used();
+  L->row_start = ar.take<uint64_t>(n + 1);
+  L->build = take_row_range_buffers(ar, n, cap);
+  const size_t build_end = ar.used();
+  ar.rewind(rows_end);
+  L->sched = take_schedule(ar, n, kept, hubs);
+  return std::max(build_end, ar.used());
+}
+
+struct RowsPlan {
+  uint64_t cap = 0;   // entries of a range's build buffers
+  bool hubs = true;   // the schedule holds the hub pass's in-lists
+};
+
+// The largest range the budget allows, with the hub in-lists if they fit
+// (the merge blocks count without them, more slowly). False when not even a
+// range of the longest row fits.
+bool plan_rows(Arena& ar, uint64_t n, uint64_t kept, uint32_t max_row, uint64_t budget, RowsPlan* plan) {
+  RowsLayout L;
+  const uint64_t lo = std::min<uint64_t>(kept, (uint64_t)max_row + 1);
+  for (bool hubs : {true, false}) {
+    if (rows_layout(ar, true, n, kept, lo, hubs, &L) > budget) continue;
+    uint64_t a = lo, b = kept;  // the largest cap in [a, b] that fits
+    while (a < b) {
+      const uint64_t m = b - (b - a) / 2;
+      if (rows_layout(ar, true, n, kept, m, hubs, &L) <= budget)
+        a = m;
+      else
+        b = m - 1;
+    }
+    plan->cap = a;
+    plan->hubs = hubs;
+    return true;
+  }
+  return false;
+}
+
+}  // namespace
+
+// Phase 2 of the rows tier: each range's rows built from its host bucket, in
+// rank order, into one resident oriented graph, which the context then holds
+// prepared (as a one-piece count leaves it) and counts once.
+void count_rows_tier(tribit_context* c, const std::vector<std::unique_ptr<uint64_t[]>>& bucket,
+                     const std::vector<uint64_t>& filled, const std::vector<uint32_t>& hb,
+                     const std::vector<uint64_t>& h_off, uint64_t n, uint64_t E, uint64_t kept, bool hubs, uint64_t cap,
+                     std::chrono::steady_clock::time_point t0, tribit_result* res) {
+  cudaStream_t st = c->st;
+  Arena& ar = c->arena;
+  RowsLayout L;
+  ar.reserve(rows_layout(ar, true, n, kept, cap, hubs, &L), false);
+  rows_layout(ar, false, n, kept, cap, hubs, &L);
+  TB_CUDA(cudaMemsetAsync(L.stats, 0, sizeof(DeviceStats), st));
+  float h2d_ms = 0.f;
+  auto upload = [&](const void* src, size_t bytes, void* dst) {
+    const auto tu = std::chrono::steady_clock::now();
+    upload_via_pinned(c, src, bytes, dst);
+    h2d_ms += ms_since(tu);
+  };
+  upload(h_off.data(), (n + 1) * sizeof(uint64_t), L.row_start);
+  const size_t P = filled.size();
+  for (size_t r = 0; r < P; ++r) {
+    if (filled[r]) upload(bucket[r].get(), filled[r] * sizeof(uint64_t), L.build.keys);
+    build_row_range(L.build, L.row_start, hb[r], hb[r + 1] - hb[r], filled[r], L.rp, L.col, L.bent, &L.stats->err,
+                    st);
+  }
+  finalize_rows(L.rp, n, L.stats, st);
+  Prepared& p = c->prep;
+  p = Prepared{};
+  p.view.n = (uint32_t)n;
+  p.view.rp = L.rp;
+  p.view.col = L.col;
+  p.view.bent = L.bent;
+  p.stats = L.stats;
+  p.n = n;
+  p.E = E;
+  c->sched = L.sched;
+  apply_dispatch(c, st);
+  c->per_graph = nullptr;
+  c->num_graphs = 0;
+  c->prepared = true;
+  TB_CUDA(cudaEventRecord(c->ev[2], st));
+  c->launch = launch_count(p.view, c->sched, p.stats, nullptr, count_config(c), st);
+  TB_CUDA(cudaEventRecord(c->ev[3], st));
+  TB_CUDA(cudaMemcpyAsync(c->h_stats, p.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, st));
+  TB_CUDA(cudaStreamSynchronize(st));
+  const DeviceStats& hs = *c->h_stats;
+  if (hs.err & kErrInput) {
+    c->prepared = false;
+    throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "the host entries changed during the count");
+  }
+  if (hs.count_err & kErrTimeout) throw StatusError(TRIBIT_ERR_TIMEOUT, "a device-side wait gave up");
+  if (!res) return;
+  std::memset(res, 0, sizeof *res);
+  fill_schedule_stats(c, res);
+  res->triangles = hs.triangles;
+  res->num_nodes = n;
+  res->entries = E;
+  res->edges = hs.edges;
+  res->blocks_of_threads = c->launch.ctas;
+  res->count_kernels = c->launch.kernels;
+  TB_CUDA(cudaEventElapsedTime(&res->kernel_ms, c->ev[2], c->ev[3]));
+  res->total_ms = ms_since(t0);
+  res->h2d_ms = h2d_ms;
+  res->preprocess_ms = std::max(0.f, res->total_ms - res->kernel_ms - h2d_ms);
+  res->stream_tasks = 1;
+  res->stream_tier = TRIBIT_STREAM_ROWS;
+}
+
 bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t E, uint64_t n, tribit_result* res) {
   DeviceGuard dg(c->device);
   if (n == 0 || E == 0) return false;
@@ -299,7 +428,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     if (pass == 0) {
       if (ar.used() > budget)
         throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the per-vertex arrays alone exceed the device budget");
-      ar.reserve(ar.used());
+      ar.reserve(ar.used(), false);
     }
   }
   ensure_pinned(c);
@@ -347,24 +476,45 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   unsigned int max_row = 0;
   check_flags(&max_row);
 
-  // ---- the ranges: a task of ranges i < j holds at most 3 cap entries
-  // (bucket i, its entries into R_j again, bucket j) on at most 2n vertices.
-  const uint64_t n2 = 2 * n;
-  const uint64_t fixed = call_bytes(c, 0, n2, TRIBIT_ORDER_ID, false);
-  const uint64_t probe = 1ull << 20;
-  const uint64_t per_entry = (call_bytes(c, probe, n2, TRIBIT_ORDER_ID, false) - fixed) / probe + 1 + sizeof(uint64_t);
-  if (budget <= fixed) throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the device budget is below a range task's per-vertex buffers");
-  const uint64_t cap = std::min<uint64_t>((budget - fixed) / per_entry / 3, 0xfffffffeull / 3);
-  if (cap <= max_row) throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the device budget is below the longest row's share");
-  const uint64_t step = cap - max_row;
-  const uint64_t P = std::max<uint64_t>(1, ceil_div<uint64_t>(kept, step));
+  // ---- the tier and its ranges -------------------------------------------------
+  // Rows tier: the oriented rows (rp, col, bent) and the schedule stay on the
+  // device, and one range's build buffers of `cap` entries come and go. Pairs
+  // tier: a task of ranges i < j holds at most 3 cap entries (bucket i, its
+  // entries into R_j again, bucket j) on at most 2n vertices.
+  const uint64_t user_cap = c->stream_range_entries;
+  if (user_cap && user_cap <= max_row)
+    throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the range bound is at or below the longest row");
+  RowsPlan plan;
+  const bool rows_tier = c->stream_tier != TRIBIT_STREAM_PAIRS && n <= 0xffffffffull && kept <= 0xfffffffeull &&
+                         plan_rows(c->arena, n, kept, max_row, budget, &plan);
+  if (c->stream_tier == TRIBIT_STREAM_ROWS && !rows_tier)
+    throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the oriented rows alone exceed the device budget");
+  uint64_t cap = 0;
+  if (rows_tier) {
+    cap = plan.cap;
+  } else {
+    const uint64_t n2 = 2 * n;
+    const uint64_t fixed = call_bytes(c, 0, n2, TRIBIT_ORDER_ID, false);
+    const uint64_t probe = 1ull << 20;
+    const uint64_t per_entry =
+        (call_bytes(c, probe, n2, TRIBIT_ORDER_ID, false) - fixed) / probe + 1 + sizeof(uint64_t);
+    if (budget <= fixed)
+      throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the device budget is below a range task's per-vertex buffers");
+    cap = std::min<uint64_t>((budget - fixed) / per_entry / 3, 0xfffffffeull / 3);
+    if (cap <= max_row) throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the device budget is below the longest row's share");
+  }
+  if (user_cap) cap = std::min(cap, user_cap);
+  const uint64_t P = cap >= kept ? 1 : ceil_div<uint64_t>(kept, cap - max_row);
   if (P > kMaxRanges) throw StatusError(TRIBIT_ERR_TOO_LARGE, "the graph needs more rank ranges than supported");
-  k_s_bounds<<<1, kMaxRanges + 1, 0, st>>>(off, n, step, (uint32_t)P, bounds, size);
+  k_s_bounds<<<1, kMaxRanges + 1, 0, st>>>(off, n, cap >= kept ? kept + 1 : cap - max_row, (uint32_t)P, bounds, size);
   TB_LAUNCH_CHECK();
   std::vector<uint32_t> hb(P + 1);
   std::vector<uint64_t> hsize(P);
   TB_CUDA(cudaMemcpyAsync(hb.data(), bounds, (P + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaMemcpyAsync(hsize.data(), size, P * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  // The rows tier builds ranges from the global row starts.
+  std::vector<uint64_t> h_off(rows_tier ? n + 1 : 0);
+  if (rows_tier) TB_CUDA(cudaMemcpyAsync(h_off.data(), off, (n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaStreamSynchronize(st));
 
   // ---- host buckets of oriented keys, one per range --------------------------
@@ -389,15 +539,24 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     TB_CUDA(cudaStreamSynchronize(st));
     const uint64_t* back = static_cast<const uint64_t*>(c->pinned[1]);
     for (uint64_t r = 0; r < P; ++r) {
-      if (filled[r] + hh[r] > hsize[r]) throw StatusError(TRIBIT_ERR_INTERNAL, "range bucket overflow");
+      if (filled[r] + hh[r] > hsize[r]) throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "the host entries changed during the count");
       host_copy(bucket[r].get() + filled[r], back + cur[r], hh[r] * sizeof(uint64_t));
       filled[r] += hh[r];
     }
   });
   check_flags(nullptr);
-  ar.release();  // phase 1 is done: its device memory goes to the tasks
+  for (uint64_t r = 0; r < P; ++r)
+    if (filled[r] != hsize[r]) throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "the host entries changed during the count");
+  ar.release();  // phase 1 is done: its device memory goes to phase 2
+  const float phase1_ms = ms_since(t0);
 
-  // ---- phase 2: every pair of ranges i <= j ------------------------------------
+  if (rows_tier) {
+    count_rows_tier(c, bucket, filled, hb, h_off, n, E, kept, plan.hubs, cap, t0, res);
+    if (res) res->stream_ranges = (uint32_t)P;
+    return true;
+  }
+
+  // ---- phase 2 of the pairs tier: every pair of ranges i <= j ------------------
   uint64_t tri = 0, edges = 0, ctas = 0, blocks = 0, tasks = 0;
   uint64_t by_variant[TRIBIT_NUM_VARIANTS] = {0, 0, 0};
   float prep_ms = 0.f, kernel_ms = 0.f, h2d_ms = 0.f;
@@ -410,7 +569,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     ar.begin(pass == 0);
     w = ar.take<uint64_t>(3 * max_bucket + 1);
     extra = ar.take<unsigned long long>(1);
-    if (pass == 0) ar.reserve(ar.used());
+    if (pass == 0) ar.reserve(ar.used(), false);
   }
   for (uint64_t i = 0; i < P; ++i) {
     for (uint64_t j = i; j < P; ++j) {
@@ -465,12 +624,13 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     res->row_blocks = blocks;
     for (int v = 0; v < TRIBIT_NUM_VARIANTS; ++v) res->row_blocks_by_variant[v] = by_variant[v];
     res->h2d_ms = h2d_ms;
-    res->preprocess_ms = prep_ms;
+    res->preprocess_ms = phase1_ms + prep_ms;
     res->kernel_ms = kernel_ms;
     res->total_ms = ms_since(t0);
     res->count_kernels = kernels;
     res->stream_ranges = (uint32_t)P;
     res->stream_tasks = (uint32_t)tasks;
+    res->stream_tier = TRIBIT_STREAM_PAIRS;
   }
   return true;
 }
@@ -480,5 +640,12 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
 extern "C" tribit_status tribit_set_device_budget(tribit_context* c, uint64_t bytes) {
   if (!c) return TRIBIT_ERR_INVALID_ARGUMENT;
   c->device_budget = bytes;
+  return TRIBIT_OK;
+}
+
+extern "C" tribit_status tribit_set_stream_options(tribit_context* c, int tier, uint64_t range_entries) {
+  if (!c || tier < TRIBIT_STREAM_AUTO || tier > TRIBIT_STREAM_PAIRS) return TRIBIT_ERR_INVALID_ARGUMENT;
+  c->stream_tier = tier;
+  c->stream_range_entries = range_entries;
   return TRIBIT_OK;
 }
