@@ -50,8 +50,11 @@ def test_streamed_counts_match_oracle(name, n, make):
             assert (r.triangles, r.edges) == want, (name, frac, r.stream_tier, r.stream_ranges)
             assert r.stream_tier in (ROWS, PAIRS)
             if r.stream_tier == ROWS:
-                # The rows tier builds the one-piece oriented graph, range by range.
-                assert r.stream_tasks == 1 and _schedule(r) == one_piece
+                # The rows tier builds the one-piece oriented graph, range by
+                # range; a small budget may leave no room for the hub in-lists
+                # (the merge blocks then count without the hub pass).
+                assert r.stream_tasks == 1 and _schedule(r)[:2] == one_piece[:2], (name, frac)
+                assert r.hub_edges in (0, one_piece[2]) and (frac < 0.8 or r.hub_edges == one_piece[2]), (name, frac)
         # Rows tier in many ranges: the same graph again.
         c.set_device_budget(int(need * 0.8))
         kept = int(np.count_nonzero((e >> np.uint64(32)) != (e & np.uint64(0xffffffff))))
@@ -146,7 +149,7 @@ def test_streamed_id_range_error_and_recovery():
 
 
 def test_stream_option_errors():
-    n, e = 1 << 12, tb.gen_rmat(12, 16, seed=5)
+    n, e = 1 << 14, tb.gen_rmat(14, 16, seed=5)
     with tb.Counter() as c:
         assert tb.lib.tribit_set_stream_options(c.handle, 7, 0) == 1  # no such tier
         c.set_device_budget(int(c.device_bytes(e.size, n) * 0.5))

@@ -2038,8 +2038,8 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.save = ar.take<unsigned long long>(n + 1);
     s.in_cnt = ar.take<uint32_t>(n + 1);
     s.in_off = ar.take<uint32_t>(n + 1);
-    s.inl = ar.take<uint64_t>(E + 1);
-    s.inrow = ar.take<uint32_t>(E + 1);
+    s.inl_cap = E + 1;
+    s.inl = ar.take<uint64_t>(s.inl_cap);
     s.hub_pieces = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
     s.hub_pieces2 = ar.take<uint64_t>(2 * n + E / kHubWarpPiece + 64);
     s.piece_wave = ar.take<uint8_t>(2 * n + E / kHubWarpPiece + 64);

@@ -57,7 +57,8 @@ struct Schedule {
   uint32_t* in_cnt = nullptr;      // device, n + 1
   uint32_t* in_off = nullptr;      // device, n + 1: in-list of hub v at [in_off[v], in_off[v+1])
   uint64_t* inl = nullptr;         // device: (first block of u's tail << 32) | tail length
-  uint32_t* inrow = nullptr;       // device: u of each in-list entry
+  uint64_t inl_cap = 0;            // entries inl (and inrow) hold
+  uint32_t* inrow = nullptr;       // device: u of each in-list entry (timing mode only: its own buffer)
   uint64_t* hub_pieces = nullptr;  // device: (v << 32) | first in-list entry; CTA pieces, then warp pieces
   uint64_t* hub_pieces2 = nullptr; // device: the pieces in hub order, before the wave sort
   uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail

@@ -512,16 +512,21 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     DeviceGuard dg(c->device);
     const uint64_t nrb = c->sched.num_row_blocks;
     if (cycles_out && cap < nrb) throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "timing buffer too small");
+    // Per-block times, and the in-list rows the hub pieces charge their
+    // cycles to (a one-piece schedule keeps no rows).
     tb::Arena& ar = c->timing_arena;
+    const bool hub_rows = variant == TRIBIT_VARIANT_MERGE && c->sched.inl;
     ar.begin(true);
     ar.take<unsigned long long>(nrb + 1);
+    if (hub_rows) ar.take<uint32_t>(c->sched.inl_cap);
     ar.reserve(ar.used());
     ar.begin(false);
     unsigned long long* ns = ar.take<unsigned long long>(nrb + 1);
+    c->sched.inrow = hub_rows ? ar.take<uint32_t>(c->sched.inl_cap) : nullptr;
     TB_CUDA(cudaMemsetAsync(ns, 0, (nrb + 1) * sizeof(unsigned long long), c->st));
     if (nrb) TB_CUDA(cudaMemsetAsync(c->sched.variant_of, variant, nrb, c->st));
     c->sched.hubs = variant == TRIBIT_VARIANT_MERGE;
-    c->sched.hub_rows = true;  // the hub pieces charge their cycles to their rows' blocks
+    c->sched.hub_rows = hub_rows;  // the hub pieces charge their cycles to their rows' blocks
     tb::build_pieces(c->prep.view, c->sched, c->st);
     c->sched.hub_rows = false;
     tb::CountConfig cfg = tb::count_config(c);
@@ -537,6 +542,7 @@ tribit_status tribit_block_times(tribit_context* c, int variant, float* cycles_o
     if (variant_ms) TB_CUDA(cudaEventElapsedTime(variant_ms, c->ev[0], c->ev[1]));
     if (cycles_out)
       for (uint64_t i = 0; i < nrb; ++i) cycles_out[i] = (float)h[i];
+    c->sched.inrow = nullptr;
     tb::apply_dispatch(c, c->st);
     TB_CUDA(cudaStreamSynchronize(c->st));
   });

@@ -46,6 +46,7 @@ constexpr int kThreads = 256;
 constexpr uint64_t kPieceWords = (32u << 20) / sizeof(uint64_t);  // entries of one pinned buffer
 constexpr uint32_t kMaxRanges = 1023;                              // one CTA computes the bounds
 constexpr uint64_t kNoKey = ~0ull;
+static_assert(kUploadChunks + 1 >= 5, "the piece streaming uses five upload events");
 
 inline unsigned grid_for(uint64_t n) {
   const uint64_t g = ceil_div<uint64_t>(n, (uint64_t)kThreads * 8);
@@ -402,11 +403,13 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
 
   // ---- phase 1: per-vertex buffers and the pieces in flight -----------------
   // A piece of at most 32 MiB of entries, and at most 1/64 of the budget (its
-  // device buffers take 28 bytes an entry).
+  // device buffers take 36 bytes an entry: two piece buffers, keys, ranges,
+  // grouped keys).
   const uint64_t piece_words = std::max<uint64_t>(1u << 16, std::min<uint64_t>(kPieceWords, budget / 64));
   Arena& ar = c->stream_arena;
   uint32_t *deg = nullptr, *rank = nullptr, *rows = nullptr, *bounds = nullptr, *hist = nullptr, *rng = nullptr;
-  uint64_t *off = nullptr, *otmp = nullptr, *size = nullptr, *piece = nullptr, *keys = nullptr, *part = nullptr;
+  uint64_t *off = nullptr, *otmp = nullptr, *size = nullptr, *keys = nullptr, *part = nullptr;
+  uint64_t* pieces[2] = {nullptr, nullptr};
   unsigned int* flags = nullptr;  // [0] error flags, [1] longest row
   RankBuffers rb;
   for (int pass = 0; pass < 2; ++pass) {
@@ -421,7 +424,8 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     size = ar.take<uint64_t>(kMaxRanges);
     hist = ar.take<uint32_t>(kMaxRanges);
     flags = ar.take<unsigned int>(2);
-    piece = ar.take<uint64_t>(piece_words);
+    pieces[0] = ar.take<uint64_t>(piece_words);
+    pieces[1] = ar.take<uint64_t>(piece_words);
     keys = ar.take<uint64_t>(piece_words);
     rng = ar.take<uint32_t>(piece_words);
     part = ar.take<uint64_t>(piece_words);
@@ -433,18 +437,48 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   }
   ensure_pinned(c);
   TB_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned int), st));
-  // Streams the host entries through `piece`, calling fn(count) per piece
-  // (host copy into a pinned buffer while the previous piece's kernels run).
+  // Streams the host entries through the two device piece buffers, calling
+  // fn(piece, count) per piece. Pinned host entries are copied straight from
+  // the caller's buffer on the copy stream, piece k + 1 while piece k's
+  // kernels run; pageable ones through the context's pinned buffers, the host
+  // copy of piece k + 1 while piece k's copy and kernels run.
+  cudaPointerAttributes pa{};
+  const bool pinned_src = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();
+  cudaEvent_t* ev = c->upload_ev;  // [1 + b]: buffer b's copy done (pageable) or its kernels done (pinned);
+                                   // [3 + b]: buffer b's copy done (pinned)
+  const uint64_t npieces = ceil_div<uint64_t>(E, piece_words);
+  auto piece_size = [&](uint64_t k) { return std::min<uint64_t>(piece_words, E - k * piece_words); };
+  auto issue_copy = [&](uint64_t k) {  // pinned source: piece k into buffer k & 1, once piece k - 2 is done
+    const int b = (int)(k & 1);
+    if (k >= 2) TB_CUDA(cudaStreamWaitEvent(c->copy_st, ev[1 + b], 0));
+    TB_CUDA(cudaMemcpyAsync(pieces[b], host + k * piece_words, piece_size(k) * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, c->copy_st));
+    TB_CUDA(cudaEventRecord(ev[3 + b], c->copy_st));
+  };
   auto stream_pass = [&](auto&& fn) {
-    uint64_t k = 0;
-    for (uint64_t at = 0; at < E; at += piece_words, ++k) {
-      const uint64_t cnt = std::min<uint64_t>(piece_words, E - at);
-      void* pin = c->pinned[k & 1];
-      if (k >= 2) TB_CUDA(cudaEventSynchronize(c->upload_ev[1 + (k & 1)]));
-      host_copy(pin, host + at, cnt * sizeof(uint64_t));
-      TB_CUDA(cudaMemcpyAsync(piece, pin, cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-      TB_CUDA(cudaEventRecord(c->upload_ev[1 + (k & 1)], st));
-      fn(cnt);
+    if (pinned_src) {  // the copies follow all earlier work on the stream
+      TB_CUDA(cudaEventRecord(ev[0], st));
+      TB_CUDA(cudaStreamWaitEvent(c->copy_st, ev[0], 0));
+      issue_copy(0);
+    }
+    for (uint64_t k = 0; k < npieces; ++k) {
+      const uint64_t at = k * piece_words, cnt = piece_size(k);
+      const int b = (int)(k & 1);
+      uint64_t* dst = pieces[b];
+      if (pinned_src) {
+        if (k + 1 < npieces) issue_copy(k + 1);  // in flight while piece k is processed
+        TB_CUDA(cudaStreamWaitEvent(st, ev[3 + b], 0));
+        fn(dst, cnt);
+        TB_CUDA(cudaEventRecord(ev[1 + b], st));
+      } else {
+        void* pin = c->pinned[b];
+        if (k >= 2) TB_CUDA(cudaEventSynchronize(ev[1 + b]));
+        host_copy(pin, host + at, cnt * sizeof(uint64_t));
+        TB_CUDA(cudaMemcpyAsync(dst, pin, cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        TB_CUDA(cudaEventRecord(ev[1 + b], st));
+        fn(dst, cnt);
+      }
     }
   };
   auto check_flags = [&](unsigned int* out2) {
@@ -456,7 +490,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   };
   // Degrees, then the (degree, id) rank order.
   TB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(uint32_t), st));
-  stream_pass([&](uint64_t cnt) {
+  stream_pass([&](const uint64_t* piece, uint64_t cnt) {
     k_s_degree<<<grid_for(cnt), kThreads, 0, st>>>(piece, cnt, n, deg, flags);
     TB_LAUNCH_CHECK();
   });
@@ -464,7 +498,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   rank_vertices(deg, n, E, rb, rank, st);
   // Oriented entries per row (with duplicates), their prefix, the longest row.
   TB_CUDA(cudaMemsetAsync(rows, 0, (n + 1) * sizeof(uint32_t), st));
-  stream_pass([&](uint64_t cnt) {
+  stream_pass([&](const uint64_t* piece, uint64_t cnt) {
     k_s_rows<<<grid_for(cnt), kThreads, 0, st>>>(piece, cnt, n, rank, rows, flags);
     TB_LAUNCH_CHECK();
   });
@@ -522,7 +556,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   std::vector<uint64_t> filled(P, 0);
   for (uint64_t r = 0; r < P; ++r) bucket[r].reset(new uint64_t[std::max<uint64_t>(hsize[r], 1)]);
   std::vector<uint32_t> hh(P), cur(P);
-  stream_pass([&](uint64_t cnt) {
+  stream_pass([&](const uint64_t* piece, uint64_t cnt) {
     TB_CUDA(cudaMemsetAsync(hist, 0, P * sizeof(uint32_t), st));
     k_s_keys<<<grid_for(cnt), kThreads, (2 * P + 1) * sizeof(uint32_t), st>>>(piece, cnt, n, rank, bounds,
                                                                                (uint32_t)P, keys, rng, hist, flags);
