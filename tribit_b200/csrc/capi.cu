@@ -221,6 +221,7 @@ tribit_status tribit_create(const tribit_options* opts, tribit_context** out) {
     for (auto& e : c->ev) TB_CUDA(cudaEventCreate(&e));
     TB_CUDA(cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking));
     for (auto& e : c->upload_ev) TB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : c->pinned_ev) TB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TB_CUDA(cudaMallocHost(&c->h_stats, sizeof(tb::DeviceStats)));
   });
   if (st != TRIBIT_OK) {
@@ -250,6 +251,8 @@ void tribit_destroy(tribit_context* c) {
       if (e) cudaEventDestroy(e);
     if (c->copy_st) cudaStreamSynchronize(c->copy_st);
     for (auto& e : c->upload_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : c->pinned_ev)
       if (e) cudaEventDestroy(e);
     if (c->copy_st) cudaStreamDestroy(c->copy_st);
     if (c->h_stats) cudaFreeHost(c->h_stats);

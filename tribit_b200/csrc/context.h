@@ -44,6 +44,7 @@ struct tribit_context {
   tb::Arena text_arena;
   tb::Arena load_arena;
   void* pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pinned_ev[2] = {};       // the last device copy that used pinned[b], on any stream
   const uint64_t* loaded_entries = nullptr;
   uint64_t loaded_E = 0, loaded_n = 0;
   bool loaded = false;
@@ -115,6 +116,11 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
 // Copies bytes of host memory to device memory through the context's two
 // pinned buffers (host threads fill one while the other's copy runs).
 void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst);
+
+// The host writes or reads pinned buffer b only once the last device copy
+// that used it has finished; every such copy is followed by pinned_used.
+inline void pinned_wait(tribit_context* c, int b) { TB_CUDA(cudaEventSynchronize(c->pinned_ev[b])); }
+inline void pinned_used(tribit_context* c, int b, cudaStream_t s) { TB_CUDA(cudaEventRecord(c->pinned_ev[b], s)); }
 
 // Launch configuration of the context's counting kernels.
 inline CountConfig count_config(const tribit_context* c) {

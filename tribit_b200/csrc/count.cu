@@ -1773,6 +1773,15 @@ __global__ void k_hub_vinfo(GraphView g, uint64_t* __restrict__ vinfo) {
 // of u's bit row of nbu entries): the tail of u is shorter than v's row and v
 // can be staged; in mode 1 also v saves at least its staging cost (the direct
 // map's span / 4 vector stores, or a hash's 2 nb slots cleared, plus nb inserts).
+// Mode 0 adds a candidate's saving only while save[v] is below that cost: the
+// decision save[v] >= cost is then the one the full sum gives (an add is
+// skipped only when the sum has already reached the cost), without one
+// atomic per in-edge on the most popular hubs.
+__device__ __forceinline__ unsigned long long hub_cost(uint32_t span, uint32_t nbv) {
+  return span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
+                             : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin;
+}
+
 template <int Mode>
 __device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo,
                                               const unsigned long long* __restrict__ save, uint32_t v,
@@ -1781,9 +1790,8 @@ __device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo
   nbv = (uint32_t)vi;
   const uint32_t span = (uint32_t)(vi >> 32);
   bool hub = nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
-  if (Mode == 1)
-    hub = hub && save[v] >= (span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
-                                                 : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin);
+  if (Mode == 1) hub = hub && save[v] >= hub_cost(span, nbv);
+  if (Mode == 0) hub = hub && *(volatile const unsigned long long*)&save[v] < hub_cost(span, nbv);
   return hub;
 }
 

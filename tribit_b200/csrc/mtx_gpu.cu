@@ -299,14 +299,15 @@ tribit_status tribit_load_mtx(tribit_context* c, const char* path, uint64_t* num
     uint64_t k = 0;
     for (uint64_t at = 0; at < B; at += tb::kPinnedPiece, ++k) {
       const size_t len = (size_t)std::min<uint64_t>(tb::kPinnedPiece, B - at);
-      char* buf = static_cast<char*>(c->pinned[k & 1]);
-      if (k >= 2) TB_CUDA(cudaEventSynchronize(c->upload_ev[1 + (k & 1)]));
+      const int b = (int)(k & 1);
+      char* buf = static_cast<char*>(c->pinned[b]);
+      tb::pinned_wait(c, b);
       if (!tb::read_piece(f.fd, buf, off0 + at, len)) {
         io_ok = false;
         break;
       }
       TB_CUDA(cudaMemcpyAsync(text + at, buf, len, cudaMemcpyHostToDevice, c->copy_st));
-      TB_CUDA(cudaEventRecord(c->upload_ev[1 + (k & 1)], c->copy_st));
+      tb::pinned_used(c, b, c->copy_st);
     }
     TB_CUDA(cudaEventRecord(c->upload_ev[3], c->copy_st));
     TB_CUDA(cudaStreamWaitEvent(s, c->upload_ev[3], 0));

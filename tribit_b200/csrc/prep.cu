@@ -507,6 +507,14 @@ __global__ void k_range_fill(const uint64_t* __restrict__ keys, uint64_t cnt, ui
   }
 }
 
+// Every row of the range got exactly its counted entries (a row short of them
+// would hold stale slots: the entries changed between passes).
+__global__ void k_range_check(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cursor, uint32_t z,
+                              unsigned int* err) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < z; k += gridDim.x * blockDim.x)
+    if (cursor[k] != off[k + 1]) atomicOr(err, kErrInput);
+}
+
 // rp[k] += *carry, k < count: the range's prefix continues the ranges before.
 __global__ void k_range_carry(uint64_t* __restrict__ rp, uint32_t count, const uint64_t* __restrict__ carry) {
   const uint64_t c = *carry;
@@ -586,11 +594,11 @@ RowRangeBuffers take_row_range_buffers(Arena& ar, uint64_t n, uint64_t cap) {
   return b;
 }
 
-void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t cnt,
-                     uint64_t* rp, uint32_t* col, uint64_t* bent, unsigned int* err, cudaStream_t st) {
+void begin_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t* rp,
+                     cudaStream_t st) {
   if (z == 0) return;
   // The ranges before this one left rp[s] = the prefix at row s, which the
-  // row sort below overwrites.
+  // row sort overwrites.
   if (s == 0)
     TB_CUDA(cudaMemsetAsync(b.carry, 0, sizeof(uint64_t), st));
   else
@@ -598,10 +606,13 @@ void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32
   TB_CUDA(cudaMemsetAsync(b.nbig, 0, sizeof(uint32_t), st));
   k_range_starts<<<grid_for((uint64_t)z + 1), kThreads, 0, st>>>(row_start, s, z, b.off, b.cursor);
   TB_LAUNCH_CHECK();
-  if (cnt > 0) {
-    k_range_fill<<<grid_for(cnt, 8), kThreads, 0, st>>>(b.keys, cnt, s, z, b.off, b.cursor, b.nbr, err);
-    TB_LAUNCH_CHECK();
-  }
+}
+
+void finish_row_range(const RowRangeBuffers& b, uint32_t s, uint32_t z, uint64_t cnt, uint64_t* rp, uint32_t* col,
+                      uint64_t* bent, unsigned int* err, cudaStream_t st) {
+  if (z == 0) return;
+  k_range_check<<<grid_for(z), kThreads, 0, st>>>(b.off, b.cursor, z, err);
+  TB_LAUNCH_CHECK();
   const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(z, 8), 148ull * 32));
   k_sort_rows<<<wgrid, kThreads, 0, st>>>(b.off, z, b.nbr, rp + s, b.big, b.nbig);
   TB_LAUNCH_CHECK();
@@ -614,6 +625,17 @@ void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32
   TB_LAUNCH_CHECK();
   k_emit_rows<<<wgrid, kThreads, 0, st>>>(b.off, b.nbr, rp + s, z, col, bent);
   TB_LAUNCH_CHECK();
+}
+
+void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t cnt,
+                     uint64_t* rp, uint32_t* col, uint64_t* bent, unsigned int* err, cudaStream_t st) {
+  if (z == 0) return;
+  begin_row_range(b, row_start, s, z, rp, st);
+  if (cnt > 0) {
+    k_range_fill<<<grid_for(cnt, 8), kThreads, 0, st>>>(b.keys, cnt, s, z, b.off, b.cursor, b.nbr, err);
+    TB_LAUNCH_CHECK();
+  }
+  finish_row_range(b, s, z, cnt, rp, col, bent, err, st);
 }
 
 void finalize_rows(const uint64_t* rp, uint64_t n, DeviceStats* stats, cudaStream_t st) {

@@ -117,6 +117,15 @@ RowRangeBuffers take_row_range_buffers(Arena& ar, uint64_t n, uint64_t cap);
 // counted and bucketed them) is dropped and sets kErrInput in *err.
 void build_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t cnt,
                      uint64_t* rp, uint32_t* col, uint64_t* bent, unsigned int* err, cudaStream_t st);
+// The same in two halves around a fill of the caller's own: begin sets the
+// range's row starts and fill cursors (b.off, b.cursor); the caller then
+// places each of the range's cnt entries at nbr[atomicAdd(&cursor[row - s], 1)]
+// (checking it against off[row - s + 1]); finish checks every row is full and
+// sorts, deduplicates and emits the rows.
+void begin_row_range(const RowRangeBuffers& b, const uint64_t* row_start, uint32_t s, uint32_t z, uint64_t* rp,
+                     cudaStream_t st);
+void finish_row_range(const RowRangeBuffers& b, uint32_t s, uint32_t z, uint64_t cnt, uint64_t* rp, uint32_t* col,
+                      uint64_t* bent, unsigned int* err, cudaStream_t st);
 // Edge and bit-block totals of rp[n] into stats.
 void finalize_rows(const uint64_t* rp, uint64_t n, DeviceStats* stats, cudaStream_t st);
 

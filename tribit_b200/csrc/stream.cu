@@ -45,6 +45,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr uint64_t kPieceWords = (32u << 20) / sizeof(uint64_t);  // entries of one pinned buffer
 constexpr uint32_t kMaxRanges = 1023;                              // one CTA computes the bounds
+// Rows tier: up to this many ranges are each filled from one more pass over
+// the host entries; more go through host buckets (one pass, keys back and up).
+constexpr uint64_t kDirectRanges = 4;
 constexpr uint64_t kNoKey = ~0ull;
 static_assert(kUploadChunks + 1 >= 5, "the piece streaming uses five upload events");
 
@@ -173,6 +176,26 @@ __global__ void k_s_scatter(const uint64_t* __restrict__ keys, const uint32_t* _
   }
 }
 
+// Rows tier, direct fill of rank range [s, s + z): every entry of the piece
+// whose lower endpoint's rank falls in the range goes to a slot of its row
+// (the range's keys never exist as such).
+__global__ void k_s_fill(const uint64_t* __restrict__ e, uint64_t cnt, uint64_t n, const uint32_t* __restrict__ rank,
+                         uint32_t s, uint32_t z, const uint32_t* __restrict__ off, uint32_t* __restrict__ cursor,
+                         uint32_t* __restrict__ nbr, unsigned int* err) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a, b;
+    if (!entry_ids(e[i], n, a, b, err)) continue;
+    const uint32_t ra = rank[a], rb = rank[b];
+    const uint32_t r = min(ra, rb) - s;
+    if (r >= z) continue;
+    const uint32_t pos = atomicAdd(&cursor[r], 1u);
+    if (pos < off[r + 1])
+      nbr[pos] = max(ra, rb);
+    else
+      atomicOr(err, kErrInput);
+  }
+}
+
 // Diagonal task: every rank r >= s becomes r - s.
 __global__ void k_s_diag(uint64_t* __restrict__ w, uint64_t cnt, uint32_t s) {
   const uint64_t d = ((uint64_t)s << 32) | s;
@@ -238,22 +261,79 @@ float ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes pa{};
+  const bool pinned = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();
+  return pinned;
+}
+
+// Host entries streamed through two device piece buffers: pass(fn) calls
+// fn(piece, count) per piece on the context's stream. Pinned host entries are
+// copied straight from the caller's buffer on the copy stream, piece k + 1
+// while piece k's work runs; pageable ones through the context's pinned
+// buffers, the host copy of piece k + 1 while piece k's copy and work run.
+struct PieceStream {
+  tribit_context* c = nullptr;
+  const uint64_t* host = nullptr;
+  uint64_t E = 0, piece_words = 0;
+  bool pinned_src = false;
+  uint64_t* pieces[2] = {nullptr, nullptr};
+
+  uint64_t size(uint64_t k) const { return std::min<uint64_t>(piece_words, E - k * piece_words); }
+  // Pinned source: upload_ev[1 + b]: buffer b's work done; upload_ev[3 + b]:
+  // buffer b's copy done.
+  void issue_copy(uint64_t k) const {
+    const int b = (int)(k & 1);
+    if (k >= 2) TB_CUDA(cudaStreamWaitEvent(c->copy_st, c->upload_ev[1 + b], 0));
+    TB_CUDA(cudaMemcpyAsync(pieces[b], host + k * piece_words, size(k) * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                            c->copy_st));
+    TB_CUDA(cudaEventRecord(c->upload_ev[3 + b], c->copy_st));
+  }
+  template <typename Fn>
+  void pass(Fn&& fn) const {
+    cudaStream_t st = c->st;
+    const uint64_t npieces = ceil_div<uint64_t>(E, piece_words);
+    if (pinned_src) {  // the copies follow all earlier work on the stream
+      TB_CUDA(cudaEventRecord(c->upload_ev[0], st));
+      TB_CUDA(cudaStreamWaitEvent(c->copy_st, c->upload_ev[0], 0));
+      if (npieces) issue_copy(0);
+    }
+    for (uint64_t k = 0; k < npieces; ++k) {
+      const uint64_t cnt = size(k);
+      const int b = (int)(k & 1);
+      if (pinned_src) {
+        if (k + 1 < npieces) issue_copy(k + 1);
+        TB_CUDA(cudaStreamWaitEvent(st, c->upload_ev[3 + b], 0));
+        fn(static_cast<const uint64_t*>(pieces[b]), cnt);
+        TB_CUDA(cudaEventRecord(c->upload_ev[1 + b], st));
+      } else {
+        void* pin = c->pinned[b];
+        pinned_wait(c, b);
+        host_copy(pin, host + k * piece_words, cnt * sizeof(uint64_t));
+        TB_CUDA(cudaMemcpyAsync(pieces[b], pin, cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        pinned_used(c, b, st);
+        fn(static_cast<const uint64_t*>(pieces[b]), cnt);
+      }
+    }
+  }
+};
+
 }  // namespace
 
 void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst) {
   ensure_pinned(c);
-  // Copies of an earlier call may still read the pinned buffers.
-  TB_CUDA(cudaStreamSynchronize(c->copy_st));
   const size_t piece = kPieceWords * sizeof(uint64_t);
   TB_CUDA(cudaEventRecord(c->upload_ev[0], c->st));
   TB_CUDA(cudaStreamWaitEvent(c->copy_st, c->upload_ev[0], 0));
   uint64_t k = 0;
   for (size_t at = 0; at < bytes; at += piece, ++k) {
     const size_t len = std::min(piece, bytes - at);
-    if (k >= 2) TB_CUDA(cudaEventSynchronize(c->upload_ev[1 + (k & 1)]));
-    host_copy(c->pinned[k & 1], (const char*)src + at, len);
-    TB_CUDA(cudaMemcpyAsync((char*)dst + at, c->pinned[k & 1], len, cudaMemcpyHostToDevice, c->copy_st));
-    TB_CUDA(cudaEventRecord(c->upload_ev[1 + (k & 1)], c->copy_st));
+    const int b = (int)(k & 1);
+    pinned_wait(c, b);
+    host_copy(c->pinned[b], (const char*)src + at, len);
+    TB_CUDA(cudaMemcpyAsync((char*)dst + at, c->pinned[b], len, cudaMemcpyHostToDevice, c->copy_st));
+    pinned_used(c, b, c->copy_st);
   }
   TB_CUDA(cudaEventRecord(c->upload_ev[3], c->copy_st));
   TB_CUDA(cudaStreamWaitEvent(c->st, c->upload_ev[3], 0));
@@ -261,20 +341,25 @@ void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* d
 
 namespace {
 
-// The rows tier's device layout: the oriented graph's rows and the row starts
-// (kept), one range's build buffers, and over those buffers (dead once the
-// rows are built) the counting schedule. Returns the arena bytes.
+// The rows tier's device layout: the oriented graph's rows (kept), then what
+// only the build uses -- the row starts, the rank of every vertex and two
+// piece buffers (for ranges filled straight from the streamed entries), one
+// range's build buffers -- and over those (dead once the rows are built) the
+// counting schedule. Returns the arena bytes.
 struct RowsLayout {
   DeviceStats* stats = nullptr;
   uint64_t* rp = nullptr;
   uint32_t* col = nullptr;
   uint64_t* bent = nullptr;
   uint64_t* row_start = nullptr;
+  uint32_t* rank = nullptr;
+  uint64_t* pieces[2] = {nullptr, nullptr};
   RowRangeBuffers build;
   Schedule sched;
 };
 
-size_t rows_layout(Arena& ar, bool measure, uint64_t n, uint64_t kept, uint64_t cap, bool hubs, RowsLayout* L) {
+size_t rows_layout(Arena& ar, bool measure, uint64_t n, uint64_t kept, uint64_t cap, bool hubs, uint64_t piece_words,
+                   RowsLayout* L) {
   ar.begin(measure);
   L->stats = ar.take<DeviceStats>(1);
   L->rp = ar.take<uint64_t>(n + 1);
@@ -282,6 +367,9 @@ size_t rows_layout(Arena& ar, bool measure, uint64_t n, uint64_t kept, uint64_t 
   L->bent = ar.take<uint64_t>(kept + 2);  // + 2: 16-byte pair loads may read one entry past the end
   const size_t rows_end = ar.used();
   L->row_start = ar.take<uint64_t>(n + 1);
+  L->rank = ar.take<uint32_t>(n);
+  L->pieces[0] = ar.take<uint64_t>(piece_words);
+  L->pieces[1] = ar.take<uint64_t>(piece_words);
   L->build = take_row_range_buffers(ar, n, cap);
   const size_t build_end = ar.used();
   ar.rewind(rows_end);
@@ -297,15 +385,16 @@ struct RowsPlan {
 // The largest range the budget allows, with the hub in-lists if they fit
 // (the merge blocks count without them, more slowly). False when not even a
 // range of the longest row fits.
-bool plan_rows(Arena& ar, uint64_t n, uint64_t kept, uint32_t max_row, uint64_t budget, RowsPlan* plan) {
+bool plan_rows(Arena& ar, uint64_t n, uint64_t kept, uint32_t max_row, uint64_t budget, uint64_t piece_words,
+               RowsPlan* plan) {
   RowsLayout L;
   const uint64_t lo = std::min<uint64_t>(kept, (uint64_t)max_row + 1);
   for (bool hubs : {true, false}) {
-    if (rows_layout(ar, true, n, kept, lo, hubs, &L) > budget) continue;
+    if (rows_layout(ar, true, n, kept, lo, hubs, piece_words, &L) > budget) continue;
     uint64_t a = lo, b = kept;  // the largest cap in [a, b] that fits
     while (a < b) {
       const uint64_t m = b - (b - a) / 2;
-      if (rows_layout(ar, true, n, kept, m, hubs, &L) <= budget)
+      if (rows_layout(ar, true, n, kept, m, hubs, piece_words, &L) <= budget)
         a = m;
       else
         b = m - 1;
@@ -319,31 +408,63 @@ bool plan_rows(Arena& ar, uint64_t n, uint64_t kept, uint32_t max_row, uint64_t 
 
 }  // namespace
 
-// Phase 2 of the rows tier: each range's rows built from its host bucket, in
-// rank order, into one resident oriented graph, which the context then holds
-// prepared (as a one-piece count leaves it) and counts once.
-void count_rows_tier(tribit_context* c, const std::vector<std::unique_ptr<uint64_t[]>>& bucket,
-                     const std::vector<uint64_t>& filled, const std::vector<uint32_t>& hb,
-                     const std::vector<uint64_t>& h_off, uint64_t n, uint64_t E, uint64_t kept, bool hubs, uint64_t cap,
+// Where the rows tier's ranges come from: host buckets of oriented keys, one
+// per range, or the host entries streamed once more per range.
+struct RowsSource {
+  const std::vector<std::unique_ptr<uint64_t[]>>* bucket = nullptr;  // null: streamed
+  const PieceStream* stream = nullptr;
+  const std::vector<uint32_t>* rank = nullptr;  // streamed: the rank of every vertex
+};
+
+// Phase 2 of the rows tier: each range's rows built in rank order into one
+// resident oriented graph, which the context then holds prepared (as a
+// one-piece count leaves it) and counts once. size[r]: range r's entries.
+void count_rows_tier(tribit_context* c, const RowsSource& src, const std::vector<uint64_t>& size,
+                     const std::vector<uint32_t>& hb, const std::vector<uint64_t>& h_off, uint64_t n, uint64_t E,
+                     uint64_t kept, bool hubs, uint64_t cap, uint64_t piece_words,
                      std::chrono::steady_clock::time_point t0, tribit_result* res) {
   cudaStream_t st = c->st;
   Arena& ar = c->arena;
   RowsLayout L;
-  ar.reserve(rows_layout(ar, true, n, kept, cap, hubs, &L), false);
-  rows_layout(ar, false, n, kept, cap, hubs, &L);
+  ar.reserve(rows_layout(ar, true, n, kept, cap, hubs, piece_words, &L), false);
+  rows_layout(ar, false, n, kept, cap, hubs, piece_words, &L);
   TB_CUDA(cudaMemsetAsync(L.stats, 0, sizeof(DeviceStats), st));
   float h2d_ms = 0.f;
-  auto upload = [&](const void* src, size_t bytes, void* dst) {
+  auto upload = [&](const void* from, size_t bytes, void* dst) {
     const auto tu = std::chrono::steady_clock::now();
-    upload_via_pinned(c, src, bytes, dst);
+    upload_via_pinned(c, from, bytes, dst);
     h2d_ms += ms_since(tu);
   };
   upload(h_off.data(), (n + 1) * sizeof(uint64_t), L.row_start);
-  const size_t P = filled.size();
+  PieceStream ps;
+  if (!src.bucket) {
+    upload(src.rank->data(), n * sizeof(uint32_t), L.rank);
+    ps = *src.stream;
+    ps.pieces[0] = L.pieces[0];
+    ps.pieces[1] = L.pieces[1];
+  }
+  const size_t P = size.size();
   for (size_t r = 0; r < P; ++r) {
-    if (filled[r]) upload(bucket[r].get(), filled[r] * sizeof(uint64_t), L.build.keys);
-    build_row_range(L.build, L.row_start, hb[r], hb[r + 1] - hb[r], filled[r], L.rp, L.col, L.bent, &L.stats->err,
-                    st);
+    const uint32_t s = hb[r], z = hb[r + 1] - hb[r];
+    if (src.bucket) {
+      if (size[r]) upload((*src.bucket)[r].get(), size[r] * sizeof(uint64_t), L.build.keys);
+      build_row_range(L.build, L.row_start, s, z, size[r], L.rp, L.col, L.bent, &L.stats->err, st);
+      continue;
+    }
+    if (z == 0) continue;
+    begin_row_range(L.build, L.row_start, s, z, L.rp, st);
+    TB_CUDA(cudaEventRecord(c->ev[0], st));
+    ps.pass([&](const uint64_t* piece, uint64_t cnt) {
+      k_s_fill<<<grid_for(cnt), kThreads, 0, st>>>(piece, cnt, n, L.rank, s, z, L.build.off, L.build.cursor,
+                                                   L.build.nbr, &L.stats->err);
+      TB_LAUNCH_CHECK();
+    });
+    TB_CUDA(cudaEventRecord(c->ev[1], st));
+    finish_row_range(L.build, s, z, size[r], L.rp, L.col, L.bent, &L.stats->err, st);
+    float pass_ms = 0.f;
+    TB_CUDA(cudaEventSynchronize(c->ev[1]));
+    TB_CUDA(cudaEventElapsedTime(&pass_ms, c->ev[0], c->ev[1]));
+    h2d_ms += pass_ms;
   }
   finalize_rows(L.rp, n, L.stats, st);
   Prepared& p = c->prep;
@@ -366,7 +487,7 @@ void count_rows_tier(tribit_context* c, const std::vector<std::unique_ptr<uint64
   TB_CUDA(cudaMemcpyAsync(c->h_stats, p.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaStreamSynchronize(st));
   const DeviceStats& hs = *c->h_stats;
-  if (hs.err & kErrInput) {
+  if (hs.err & (kErrInput | kErrIdRange)) {
     c->prepared = false;
     throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "the host entries changed during the count");
   }
@@ -402,10 +523,10 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   c->prepared = false;
 
   // ---- phase 1: per-vertex buffers and the pieces in flight -----------------
-  // A piece of at most 32 MiB of entries, and at most 1/64 of the budget (its
-  // device buffers take 36 bytes an entry: two piece buffers, keys, ranges,
-  // grouped keys).
-  const uint64_t piece_words = std::max<uint64_t>(1u << 16, std::min<uint64_t>(kPieceWords, budget / 64));
+  // A piece of at most 32 MiB of entries and at most 1/2048 of the budget in
+  // entries (phase 1's piece buffers take 36 bytes an entry: two piece
+  // buffers, keys, ranges, grouped keys; the rows tier's two take 16).
+  const uint64_t piece_words = std::max<uint64_t>(1u << 14, std::min<uint64_t>(kPieceWords, budget / 2048));
   Arena& ar = c->stream_arena;
   uint32_t *deg = nullptr, *rank = nullptr, *rows = nullptr, *bounds = nullptr, *hist = nullptr, *rng = nullptr;
   uint64_t *off = nullptr, *otmp = nullptr, *size = nullptr, *keys = nullptr, *part = nullptr;
@@ -437,50 +558,15 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   }
   ensure_pinned(c);
   TB_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned int), st));
-  // Streams the host entries through the two device piece buffers, calling
-  // fn(piece, count) per piece. Pinned host entries are copied straight from
-  // the caller's buffer on the copy stream, piece k + 1 while piece k's
-  // kernels run; pageable ones through the context's pinned buffers, the host
-  // copy of piece k + 1 while piece k's copy and kernels run.
-  cudaPointerAttributes pa{};
-  const bool pinned_src = cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-  (void)cudaGetLastError();
-  cudaEvent_t* ev = c->upload_ev;  // [1 + b]: buffer b's copy done (pageable) or its kernels done (pinned);
-                                   // [3 + b]: buffer b's copy done (pinned)
-  const uint64_t npieces = ceil_div<uint64_t>(E, piece_words);
-  auto piece_size = [&](uint64_t k) { return std::min<uint64_t>(piece_words, E - k * piece_words); };
-  auto issue_copy = [&](uint64_t k) {  // pinned source: piece k into buffer k & 1, once piece k - 2 is done
-    const int b = (int)(k & 1);
-    if (k >= 2) TB_CUDA(cudaStreamWaitEvent(c->copy_st, ev[1 + b], 0));
-    TB_CUDA(cudaMemcpyAsync(pieces[b], host + k * piece_words, piece_size(k) * sizeof(uint64_t),
-                            cudaMemcpyHostToDevice, c->copy_st));
-    TB_CUDA(cudaEventRecord(ev[3 + b], c->copy_st));
-  };
-  auto stream_pass = [&](auto&& fn) {
-    if (pinned_src) {  // the copies follow all earlier work on the stream
-      TB_CUDA(cudaEventRecord(ev[0], st));
-      TB_CUDA(cudaStreamWaitEvent(c->copy_st, ev[0], 0));
-      issue_copy(0);
-    }
-    for (uint64_t k = 0; k < npieces; ++k) {
-      const uint64_t at = k * piece_words, cnt = piece_size(k);
-      const int b = (int)(k & 1);
-      uint64_t* dst = pieces[b];
-      if (pinned_src) {
-        if (k + 1 < npieces) issue_copy(k + 1);  // in flight while piece k is processed
-        TB_CUDA(cudaStreamWaitEvent(st, ev[3 + b], 0));
-        fn(dst, cnt);
-        TB_CUDA(cudaEventRecord(ev[1 + b], st));
-      } else {
-        void* pin = c->pinned[b];
-        if (k >= 2) TB_CUDA(cudaEventSynchronize(ev[1 + b]));
-        host_copy(pin, host + at, cnt * sizeof(uint64_t));
-        TB_CUDA(cudaMemcpyAsync(dst, pin, cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        TB_CUDA(cudaEventRecord(ev[1 + b], st));
-        fn(dst, cnt);
-      }
-    }
-  };
+  PieceStream ps;
+  ps.c = c;
+  ps.host = host;
+  ps.E = E;
+  ps.piece_words = piece_words;
+  ps.pinned_src = host_is_pinned(host);
+  ps.pieces[0] = pieces[0];
+  ps.pieces[1] = pieces[1];
+  auto stream_pass = [&](auto&& fn) { ps.pass(fn); };
   auto check_flags = [&](unsigned int* out2) {
     unsigned int h[2] = {0, 0};
     TB_CUDA(cudaMemcpyAsync(h, flags, sizeof h, cudaMemcpyDeviceToHost, st));
@@ -520,7 +606,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the range bound is at or below the longest row");
   RowsPlan plan;
   const bool rows_tier = c->stream_tier != TRIBIT_STREAM_PAIRS && n <= 0xffffffffull && kept <= 0xfffffffeull &&
-                         plan_rows(c->arena, n, kept, max_row, budget, &plan);
+                         plan_rows(c->arena, n, kept, max_row, budget, piece_words, &plan);
   if (c->stream_tier == TRIBIT_STREAM_ROWS && !rows_tier)
     throw StatusError(TRIBIT_ERR_OUT_OF_MEMORY, "the oriented rows alone exceed the device budget");
   uint64_t cap = 0;
@@ -546,10 +632,25 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   std::vector<uint64_t> hsize(P);
   TB_CUDA(cudaMemcpyAsync(hb.data(), bounds, (P + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaMemcpyAsync(hsize.data(), size, P * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  // The rows tier builds ranges from the global row starts.
+  // The rows tier builds ranges from the global row starts; with few ranges
+  // it fills each one straight from the entries streamed again (the ranks
+  // orient them), instead of sending every key to a host bucket and back.
+  const bool direct = rows_tier && P <= kDirectRanges;
   std::vector<uint64_t> h_off(rows_tier ? n + 1 : 0);
+  std::vector<uint32_t> h_rank(direct ? n : 0);
   if (rows_tier) TB_CUDA(cudaMemcpyAsync(h_off.data(), off, (n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  if (direct) TB_CUDA(cudaMemcpyAsync(h_rank.data(), rank, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaStreamSynchronize(st));
+
+  if (direct) {
+    ar.release();  // phase 1 is done: its device memory goes to phase 2
+    RowsSource src;
+    src.stream = &ps;
+    src.rank = &h_rank;
+    count_rows_tier(c, src, hsize, hb, h_off, n, E, kept, plan.hubs, cap, piece_words, t0, res);
+    if (res) res->stream_ranges = (uint32_t)P;
+    return true;
+  }
 
   // ---- host buckets of oriented keys, one per range --------------------------
   std::vector<std::unique_ptr<uint64_t[]>> bucket(P);
@@ -569,7 +670,9 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     k_s_scatter<<<grid_for(cnt), kThreads, 0, st>>>(keys, rng, cnt, hist, part);
     TB_LAUNCH_CHECK();
     // The grouped keys come back through pinned buffer 1 (buffer 0 may hold the next piece).
+    pinned_wait(c, 1);
     TB_CUDA(cudaMemcpyAsync(c->pinned[1], part, run * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    pinned_used(c, 1, st);
     TB_CUDA(cudaStreamSynchronize(st));
     const uint64_t* back = static_cast<const uint64_t*>(c->pinned[1]);
     for (uint64_t r = 0; r < P; ++r) {
@@ -585,7 +688,9 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   const float phase1_ms = ms_since(t0);
 
   if (rows_tier) {
-    count_rows_tier(c, bucket, filled, hb, h_off, n, E, kept, plan.hubs, cap, t0, res);
+    RowsSource src;
+    src.bucket = &bucket;
+    count_rows_tier(c, src, hsize, hb, h_off, n, E, kept, plan.hubs, cap, piece_words, t0, res);
     if (res) res->stream_ranges = (uint32_t)P;
     return true;
   }
