@@ -343,6 +343,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
+    ap.add_argument("--stream-budgets", default="0.5,0.3",
+                    help="device budgets (fractions of the one-piece need) for the out-of-HBM end-to-end "
+                         "measurement; empty to skip")
     ap.add_argument("--tile-engine", default="tcgen05", choices=["mma_sync", "tcgen05"],
                     help="arithmetic of the bit-tile variant")
     ap.add_argument("--ref-binary", default="rmat22", choices=["none"] + sorted(WORKLOADS),
@@ -467,6 +470,31 @@ def main():
         t_plain, _ = e2e_run("plain")
         e2e_by_mode["plain"] = job_edges / t_plain
 
+    def streamed_run(frac):
+        # The same call with a device budget below what a one-piece count
+        # needs: the graph is counted in rank ranges (out-of-HBM path).
+        c = tb.Counter(device=local, dispatch=dispatch)
+        if dispatch == "learned":
+            c.load_model(model_path)
+        need = c.device_bytes(entries.size, n)
+        c.set_device_budget(int(need * frac))
+        c.count_edges(host, n)
+        secs, last = [], None
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            last = c.count_edges(host, n)
+            secs.append(time.perf_counter() - t1)
+        c.close()
+        assert last.triangles == res.triangles
+        t = reduce_replicas(dist, m, statistics.mean(secs), device)[1]
+        return {"budget_frac": frac, "budget_gb": round(need * frac / 1e9, 3), "one_piece_gb": round(need / 1e9, 3),
+                "tier": ("one piece", "rows", "pairs")[last.stream_tier], "ranges": last.stream_ranges,
+                "tasks": last.stream_tasks, "value": job_edges / t, "ms_per_step": t * 1e3,
+                "count_ms": last.kernel_ms, "hub_edges": last.hub_edges}
+
+    streamed = [streamed_run(float(f)) for f in args.stream_budgets.split(",") if f.strip()]
+
     peak, peak_kind = measured_peaks()
     b_alg = 4 * (n + 1) + 4 * m
     achieved = b_alg / (ms_per_step / 1e3) / 1e9
@@ -515,7 +543,8 @@ def main():
                     # device-timed parts of the last call (the degree pass overlaps the upload)
                     "parts_ms": {"h2d": e2e_res.h2d_ms, "preprocess": e2e_res.preprocess_ms,
                                  "count": e2e_res.kernel_ms},
-                    "per_mode_edges_per_s": e2e_by_mode},
+                    "per_mode_edges_per_s": e2e_by_mode,
+                    "streamed": streamed},
             "clocks": clk,
             "gpu_launches": args.steps * res.count_kernels,
         }
