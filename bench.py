@@ -344,8 +344,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
     ap.add_argument("--stream-budgets", default="0.5,0.3",
-                    help="device budgets (fractions of the one-piece need) for the out-of-HBM end-to-end "
-                         "measurement; empty to skip")
+                    help="device budgets (fractions of the one-piece need, each optionally ':rows' or ':pairs' "
+                         "to force a tier) for the out-of-HBM end-to-end measurement; empty to skip")
+    ap.add_argument("--stream-pageable", action="store_true",
+                    help="the out-of-HBM measurement reads pageable host entries instead of pinned ones")
     ap.add_argument("--tile-engine", default="tcgen05", choices=["mma_sync", "tcgen05"],
                     help="arithmetic of the bit-tile variant")
     ap.add_argument("--ref-binary", default="rmat22", choices=["none"] + sorted(WORKLOADS),
@@ -470,30 +472,35 @@ def main():
         t_plain, _ = e2e_run("plain")
         e2e_by_mode["plain"] = job_edges / t_plain
 
-    def streamed_run(frac):
+    def streamed_run(item):
         # The same call with a device budget below what a one-piece count
         # needs: the graph is counted in rank ranges (out-of-HBM path).
+        frac, _, tier = item.partition(":")
+        frac = float(frac)
+        src = entries if args.stream_pageable else host
         c = tb.Counter(device=local, dispatch=dispatch)
         if dispatch == "learned":
             c.load_model(model_path)
         need = c.device_bytes(entries.size, n)
         c.set_device_budget(int(need * frac))
-        c.count_edges(host, n)
+        c.set_stream_options(tier or "auto", 0)
+        c.count_edges(src, n)
         secs, last = [], None
         for _ in range(2):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            last = c.count_edges(host, n)
+            last = c.count_edges(src, n)
             secs.append(time.perf_counter() - t1)
         c.close()
         assert last.triangles == res.triangles
         t = reduce_replicas(dist, m, statistics.mean(secs), device)[1]
-        return {"budget_frac": frac, "budget_gb": round(need * frac / 1e9, 3), "one_piece_gb": round(need / 1e9, 3),
+        return {"budget_frac": frac, "forced_tier": tier or None, "pinned": not args.stream_pageable,
+                "budget_gb": round(need * frac / 1e9, 3), "one_piece_gb": round(need / 1e9, 3),
                 "tier": ("one piece", "rows", "pairs")[last.stream_tier], "ranges": last.stream_ranges,
                 "tasks": last.stream_tasks, "value": job_edges / t, "ms_per_step": t * 1e3,
                 "count_ms": last.kernel_ms, "hub_edges": last.hub_edges}
 
-    streamed = [streamed_run(float(f)) for f in args.stream_budgets.split(",") if f.strip()]
+    streamed = [streamed_run(f.strip()) for f in args.stream_budgets.split(",") if f.strip()]
 
     peak, peak_kind = measured_peaks()
     b_alg = 4 * (n + 1) + 4 * m
