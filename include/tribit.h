@@ -262,19 +262,23 @@ tribit_status tribit_count_batch(tribit_context* ctx, const uint64_t* entries, c
  * reserves 95% of free memory at start-up), or a latency-bound loop that must
  * not pay the implicit synchronisation of cudaMalloc / cudaFree.
  * Counts the graph in d_entries (device memory, zipped words as for
- * tribit_count_edges; degree order; bit tiles or the bitmap sweep, without the
- * merge variant's hub lists, which do not fit the scratch: on power-law graphs
- * the counting kernels then run 2-3 times longer than a context's learned
- * dispatch) on `stream` (a
+ * tribit_count_edges; degree order; the plain dispatch rule over bit tiles,
+ * the bitmap sweep and the merge variant with its hub lists, as a context's
+ * TRIBIT_DISPATCH_PLAIN does, when the hub lists fit the scratch; else bit
+ * tiles and the bitmap sweep only, which on power-law graphs take 2-3 times
+ * longer) on `stream` (a
  * cudaStream_t; NULL = the legacy default stream), taking every intermediate
  * buffer from one fixed scratch array compiled into the library
  * (tribit_noalloc_scratch_bytes() = 32 MiB, held on each device that loads it
  * until exit). Allocates no device or host memory and needs no context.
  * Asynchronous: when the stream reaches the end of the work, d_result (device,
  * 4 x uint64) holds [0] triangles, [1] undirected edges, [2] error flags
- * (TRIBIT_NOALLOC_FLAG_*; any flag set means [0] is not a valid count), [3] 0.
+ * (TRIBIT_NOALLOC_FLAG_*; any flag set means [0] is not a valid count), [3] 1
+ * when the hub lists fitted (the merge variant was open to the plain rule),
+ * else 0.
  * Returns TRIBIT_ERR_TOO_LARGE, launching nothing, for a graph whose buffers
- * do not fit the scratch array (roughly 25 bytes per entry + 80 per vertex).
+ * do not fit the scratch array (roughly 25 bytes per entry + 80 per vertex
+ * without the hub lists, 33 + 155 with them).
  * The first call on a device looks up the array's device address: make it
  * before capturing stream work on that device. All calls share the array, so
  * calls whose GPU work overlaps race: order them on one stream. */

@@ -28,6 +28,7 @@ def _graphs():
         (7115, tb.gen_chung_lu(7115, 115300, 2.0, 1000.0, seed=1)),  # ~100.8k edges
         (1 << 14, tb.gen_rmat(14, 16, seed=14)),
         (5000, tb.gen_er(5000, 60000, seed=4)),
+        (1 << 16, tb.gen_rmat(16, 16, seed=16)),  # ~1.05M entries: too large for the hub lists
     ]
 
 
@@ -39,6 +40,7 @@ def test_noalloc_matches_counted_entry_point_twice():
     assert [(w.triangles, w.edges) for w in want] == [oracle.count(e, n) for n, e in graphs]
     stream = torch.cuda.Stream()
     out = torch.empty(4, dtype=torch.int64, device="cuda")
+    hub_lists = set()
     for call in range(2):
         for (n, e), w in zip(graphs, want):
             d = torch.from_numpy(e.view(np.int64)).cuda()
@@ -48,6 +50,9 @@ def test_noalloc_matches_counted_entry_point_twice():
             stream.synchronize()
             r = out.cpu().numpy().view(np.uint64)
             assert (int(r[0]), int(r[1]), int(r[2])) == (w.triangles, w.edges, 0), (call, n)
+            hub_lists.add((n, int(r[3])))
+    # The small graphs run with the merge variant's hub lists, the largest without.
+    assert (1 << 14, 1) in hub_lists and (1 << 16, 0) in hub_lists, hub_lists
 
 
 def test_noalloc_flags_bad_ids_and_refuses_oversized_graphs():

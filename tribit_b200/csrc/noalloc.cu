@@ -48,11 +48,11 @@ static_assert((uint32_t)tb::kErrIdRange == (uint32_t)TRIBIT_NOALLOC_FLAG_ID_RANG
                   (uint32_t)tb::kErrTimeout == (uint32_t)TRIBIT_NOALLOC_FLAG_TIMEOUT,
               "d_result[2] carries the device flags as the header documents them");
 
-__global__ void k_noalloc_result(const tb::DeviceStats* stats, unsigned long long* out) {
+__global__ void k_noalloc_result(const tb::DeviceStats* stats, bool hubs, unsigned long long* out) {
   out[0] = stats->triangles;
   out[1] = stats->edges;
   out[2] = stats->err | stats->count_err;
-  out[3] = 0ull;
+  out[3] = hubs ? 1ull : 0ull;
 }
 
 }  // namespace
@@ -98,23 +98,29 @@ extern "C" tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, u
     in.E = n_entries;
     in.n = num_nodes;
     in.order = TRIBIT_ORDER_DEGREE;
-    // Layout pass: launches nothing; rejects graphs that do not fit.
-    ar.begin(true);
-    {
+    // Layout pass: launches nothing. The merge variant's hub lists (and the
+    // full features the plain rule needs to choose merge) when they fit the
+    // scratch; else bit tiles and the bitmap sweep only. Rejects graphs that
+    // fit neither way.
+    bool hubs = true;
+    for (;;) {
+      ar.begin(true);
       tb::Prepared probe;
       tb::prepare_graph(ar, in, st, &probe);
-      (void)tb::take_schedule(ar, num_nodes, n_entries, false);
+      (void)tb::take_schedule(ar, num_nodes, n_entries, hubs);
+      if (!hubs || ar.used() <= kNoAllocScratchBytes) break;
+      hubs = false;
     }
     ar.reserve(ar.used());
     ar.begin(false);
     tb::Prepared prep;
     tb::prepare_graph(ar, in, st, &prep);
-    tb::Schedule sched = tb::take_schedule(ar, num_nodes, n_entries, false);
-    tb::build_schedule(prep.view, sched, TRIBIT_DISPATCH_PLAIN, false, st);
+    tb::Schedule sched = tb::take_schedule(ar, num_nodes, n_entries, hubs);
+    tb::build_schedule(prep.view, sched, TRIBIT_DISPATCH_PLAIN, hubs, st);
     tb::CountConfig cfg;
     cfg.num_sms = sms;
     tb::launch_count(prep.view, sched, prep.stats, nullptr, cfg, st);
-    k_noalloc_result<<<1, 1, 0, st>>>(prep.stats, reinterpret_cast<unsigned long long*>(d_result));
+    k_noalloc_result<<<1, 1, 0, st>>>(prep.stats, hubs, reinterpret_cast<unsigned long long*>(d_result));
     TB_LAUNCH_CHECK();
   } catch (const tb::StatusError& e) {
     return e.status;
