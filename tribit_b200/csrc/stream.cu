@@ -46,8 +46,11 @@ constexpr int kThreads = 256;
 constexpr uint64_t kPieceWords = (32u << 20) / sizeof(uint64_t);  // entries of one pinned buffer
 constexpr uint32_t kMaxRanges = 1023;                              // one CTA computes the bounds
 // Rows tier: up to this many ranges are each filled from one more pass over
-// the host entries; more go through host buckets (one pass, keys back and up).
-constexpr uint64_t kDirectRanges = 4;
+// the host entries (pinned, copied as they are; pageable, through host
+// copies to the staging buffers); more go through host buckets (one pass,
+// keys back and up).
+constexpr uint64_t kDirectRangesPinned = 4;
+constexpr uint64_t kDirectRangesPageable = 2;
 constexpr uint64_t kNoKey = ~0ull;
 static_assert(kUploadChunks + 1 >= 5, "the piece streaming uses five upload events");
 
@@ -635,7 +638,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   // The rows tier builds ranges from the global row starts; with few ranges
   // it fills each one straight from the entries streamed again (the ranks
   // orient them), instead of sending every key to a host bucket and back.
-  const bool direct = rows_tier && P <= kDirectRanges;
+  const bool direct = rows_tier && P <= (ps.pinned_src ? kDirectRangesPinned : kDirectRangesPageable);
   std::vector<uint64_t> h_off(rows_tier ? n + 1 : 0);
   std::vector<uint32_t> h_rank(direct ? n : 0);
   if (rows_tier) TB_CUDA(cudaMemcpyAsync(h_off.data(), off, (n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
