@@ -184,8 +184,9 @@ def cpu_baseline(entries, n, m, target_s=15.0, steps=1):
         t, s = g.count_sample(threads, stride, k % stride)
         full_s = s * stride
         out.append({"value": m / full_s, "seconds": s, "stride": stride, "offset": k % stride, "sample_triangles": t})
+    work = g.work()
     g.close()
-    return out, threads
+    return out, threads, work
 
 
 def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=4096, seed=4096, steps=5,
@@ -310,7 +311,7 @@ def run_reference(args, spec, rank, world):
     import oracle
     n, e = reference_graph(spec)
     edges = int(len(oracle.fold_dedup(e.copy())))
-    steps, threads = cpu_baseline(e, n, edges, steps=args.warmup + args.steps)
+    steps, threads, _ = cpu_baseline(e, n, edges, steps=args.warmup + args.steps)
     timed = steps[args.warmup:]
     value = statistics.mean(x["value"] for x in timed)
     per_step_s = edges / value
@@ -518,11 +519,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        steps, threads = cpu_baseline(entries, n, m, steps=1)
+        steps, threads, work = cpu_baseline(entries, n, m, steps=1)
         x = steps[0]
         cpu = {"value": x["value"], "unit": "edges/s", "cores": threads, "kind": "port",
                "sample": f"oracle merge count of 32-row blocks b % {x['stride']} == 0 of the degree-ordered CSR "
-                         f"({x['seconds']:.1f} s), time x {x['stride']}"}
+                         f"({x['seconds']:.1f} s), time x {x['stride']}",
+               # element reads of a sorted-merge count on the degree-ordered CSR, and per second of the GPU count
+               "work_elements": work, "work_elements_per_s_gpu": work / (ms_per_step / 1e3)}
 
     if rank == 0:
         line = {

@@ -118,6 +118,16 @@ class CSR:
         t = _lib.oracle_count_csr_sample(ctypes.byref(self._g), threads, stride, offset, ctypes.byref(s))
         return int(t), s.value
 
+    def work(self) -> int:
+        """W = sum over oriented edges (u, v) of d+(u) + d+(v): the element
+        reads of a sorted-merge count on this CSR."""
+        if self.m == 0:
+            return 0
+        rp = np.ctypeslib.as_array(self._g.row_ptr, shape=(self.n + 1,))
+        col = np.ctypeslib.as_array(self._g.col, shape=(self.m,))
+        d = np.diff(rp).astype(np.uint64)
+        return int((d * d).sum() + d[col].sum())
+
     def row_counts(self) -> np.ndarray:
         out = np.zeros(self.n, dtype=np.uint64)
         _lib.oracle_count_rows(ctypes.byref(self._g), out.ctypes.data)

@@ -124,3 +124,19 @@ def test_oracle_rmat_generator_matches_product(scale, ef, seed):
     want = tb.gen_rmat(scale, ef, seed=seed)
     for threads in (1, 3, 8):
         np.testing.assert_array_equal(oracle.gen_rmat(scale, ef, seed=seed, threads=threads), want)
+
+
+def test_merge_work_figure():
+    # W = sum over oriented edges (u, v) of d+(u) + d+(v), from the CSR's own
+    # rows, against the same sum taken edge by edge in Python.
+    rng = np.random.default_rng(9)
+    n = 300
+    a = rng.integers(0, n, 4000, dtype=np.uint64)
+    b = rng.integers(0, n, 4000, dtype=np.uint64)
+    g = oracle.CSR(zip_pairs(zip(a, b)), n, order=1)
+    rp = np.ctypeslib.as_array(g._g.row_ptr, shape=(n + 1,)).copy()
+    col = np.ctypeslib.as_array(g._g.col, shape=(g.m,)).copy()
+    d = np.diff(rp)
+    want = sum(int(d[u]) + int(d[v]) for u in range(n) for v in col[rp[u]:rp[u + 1]])
+    assert g.work() == want and want > 0
+    g.close()
