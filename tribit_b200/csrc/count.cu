@@ -1261,6 +1261,15 @@ constexpr int kHubDepth = TB_HUB_DEPTH;         // tail blocks in flight per lan
 #define TB_HUB_PAIRS 1
 #endif
 constexpr bool kHubPairs = TB_HUB_PAIRS != 0;   // tails read as 16-byte pairs of entries
+// A hub tail holding at most TB_HUB_COL_RATIO / 100 neighbours a bit block is
+// walked as u's column ids after v (4 bytes a neighbour) instead of its bit-row
+// entries (8 bytes a block); 0 walks every tail as bit rows. Each hub's
+// in-list holds its bit-row tails first (in_cnt[v] of them), then its column
+// tails. 1.75 measured best on RMAT-24 and RMAT-22 (1.0 to 3.0 swept).
+#ifndef TB_HUB_COL_RATIO
+#define TB_HUB_COL_RATIO 175
+#endif
+constexpr uint32_t kHubColRatio = TB_HUB_COL_RATIO;
 
 // Walks the tails of in-list entries [cs, ce) (at list) against v's staged row:
 // direct-mapped masks over blocks [bmin, bmin + span) in map, or a bucketed
@@ -1342,6 +1351,92 @@ __device__ __forceinline__ uint64_t sweep_tail_pairs(const GraphView& g, const u
   return acc;
 }
 
+// Column id w as a one-bit entry of its block; `keep` false: the block alone
+// (matches nothing).
+__device__ __forceinline__ uint64_t col_entry(uint32_t w, bool keep) {
+  return ((uint64_t)(w >> 5) << 32) | (keep ? 1u << (w & 31) : 0u);
+}
+
+// Column tails (in-list entries (first CSR position << 32) | neighbours): u's
+// neighbours after v, read as aligned 16-byte quads of column ids (the col
+// array has three ids of padding past its end), each id probing v's staged
+// row as a one-bit entry. Chunks of short tails keep the per-item sweep.
+template <int DepthQuads, class Probe>
+__device__ __forceinline__ uint64_t sweep_col_quads(const GraphView& g, const uint64_t* __restrict__ list,
+                                                    uint32_t cs, uint32_t ce, const Probe& probe, uint32_t* wsm) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint4* __restrict__ quads = reinterpret_cast<const uint4*>(g.col);
+  uint64_t acc = 0;
+  for (uint32_t c = cs; c < ce; c += 32) {
+    const uint32_t j = c + lane;
+    uint32_t ib = 0, il = 0;
+    if (j < ce) {
+      const uint64_t x = list[j];
+      ib = (uint32_t)(x >> 32);
+      il = (uint32_t)x;
+    }
+    const uint32_t items = warp_sum(il);
+    if (items < 32 * 8) {
+      acc += sweep_runs<2 * DepthQuads, 8>(
+          c, min(c + 32, ce), 0, 1,
+          [&](uint32_t i, uint32_t& b, uint32_t& l) {
+            const uint64_t x = list[i];
+            b = (uint32_t)(x >> 32);
+            l = (uint32_t)x;
+          },
+          [&](uint32_t k) -> uint64_t { return col_entry(g.col[k], true); }, probe, wsm);
+      continue;
+    }
+    const uint32_t ie = ib + il;
+    const uint32_t q0 = ib >> 2, qn = il ? ((ie + 3) >> 2) - q0 : 0u;  // quads covering [ib, ie)
+    const uint32_t incl = warp_inclusive_sum(qn);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    __syncwarp();
+    wsm[lane] = incl;
+    wsm[32 + lane] = q0 - (incl - qn);  // quad t of the chunk, owned by slot s, is quad off_s + t
+    wsm[64 + lane] = ib;
+    wsm[96 + lane] = ie;
+    __syncwarp();
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t st = 16; st >= 1; st >>= 1)
+      if (wsm[s + st - 1] <= lane) s += st;
+    uint32_t lim = wsm[s], off = wsm[32 + s], lo = wsm[64 + s], hi = wsm[96 + s];
+    uint32_t racc = 0;
+    for (uint32_t base = 0; base < total; base += 32 * DepthQuads) {
+      uint4 x[DepthQuads];
+      uint32_t keep[DepthQuads];  // bit i: id i of the quad lies in the tail
+#pragma unroll
+      for (int r = 0; r < DepthQuads; ++r) {
+        const uint32_t t = base + 32 * r + lane;
+        while (t >= lim && s < 31) {
+          ++s;
+          lim = wsm[s];
+          off = wsm[32 + s];
+          lo = wsm[64 + s];
+          hi = wsm[96 + s];
+        }
+        x[r] = make_uint4(0u, 0u, 0u, 0u);
+        keep[r] = 0u;
+        if (t < total) {
+          const uint32_t q = off + t, k = 4 * q;
+          x[r] = quads[q];
+          // ids [k, k + 4) within [lo, hi): 15 << 0..3 trimmed at both ends
+          const uint32_t first = lo > k ? lo - k : 0u, last = hi - k < 4u ? hi - k : 4u;
+          keep[r] = (0xFu >> (4u - last)) & (0xFu << first);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < DepthQuads; ++r)
+        racc += probe(col_entry(x[r].x, keep[r] & 1u)) + probe(col_entry(x[r].y, keep[r] & 2u)) +
+                probe(col_entry(x[r].z, keep[r] & 4u)) + probe(col_entry(x[r].w, keep[r] & 8u));
+    }
+    acc += racc;
+  }
+  __syncwarp();
+  return acc;
+}
+
 // v's row staged as direct-mapped masks over blocks [bmin, bmin + span), with
 // map[span] = 0: a block outside the span reads that zero word instead of
 // taking a branch.
@@ -1376,9 +1471,20 @@ __device__ __forceinline__ uint64_t hub_sweep(const GraphView& g, const uint64_t
   return sweep_runs<kHubDepth, 8>(cs, ce, 0, 1, desc, load, probe, wsm);
 }
 
+// Column tails [cs, ce) of the list against v's staged row (see sweep_col_quads).
+__device__ __forceinline__ uint64_t hub_sweep_col(const GraphView& g, const uint64_t* __restrict__ list, uint32_t cs,
+                                                  uint32_t ce, bool direct, const uint32_t* map, uint32_t bmin,
+                                                  uint32_t bmax, int logb, uint32_t* wsm) {
+  if (cs >= ce) return 0;  // uniform across the warp
+  if (direct) return sweep_col_quads<kHubDepth / 2>(g, list, cs, ce, DirectProbe{map, bmin, bmax - bmin + 1}, wsm);
+  const BitmapProbe probe{reinterpret_cast<const uint64_t*>(map), logb, bmin, bmax};
+  return sweep_col_quads<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
+}
+
 __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
                                                         const uint32_t* __restrict__ piece_off,
                                                         const uint32_t* __restrict__ in_off,
+                                                        const uint32_t* __restrict__ in_bits,
                                                         const uint64_t* __restrict__ inl,
                                                         const uint32_t* __restrict__ inrow, DeviceStats* stats,
                                                         unsigned long long* per_graph,
@@ -1456,7 +1562,11 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     };
     const uint32_t cs = first_at((uint32_t)((uint64_t)tot * w / kHubWarps));
     const uint32_t ce = w + 1 == kHubWarps ? cnt : first_at((uint32_t)((uint64_t)tot * (w + 1) / kHubWarps));
-    const uint64_t racc = hub_sweep(g, inl + e0, cs, ce, direct, map, bmin, bmax, logb, runs[w]);
+    // Entries before nbits are bit-row tails, the rest column tails.
+    const uint32_t nbits = kHubColRatio ? min(cnt, in_off[v] + in_bits[v] - min(e0, in_off[v] + in_bits[v]))
+                                        : cnt;
+    uint64_t racc = hub_sweep(g, inl + e0, cs, min(ce, nbits), direct, map, bmin, bmax, logb, runs[w]);
+    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, max(cs, nbits), ce, direct, map, bmin, bmax, logb, runs[w]);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -1506,7 +1616,10 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
       table_insert(wtbl, logb, g.bent, bs, be, lane, 32);
     }
     __syncwarp();
-    const uint64_t racc = hub_sweep(g, inl + e0, 0, cnt, direct, wmap, bmin, bmax, logb, runs[w]);
+    const uint32_t nbits = kHubColRatio ? min(cnt, in_off[v] + in_bits[v] - min(e0, in_off[v] + in_bits[v]))
+                                        : cnt;
+    uint64_t racc = hub_sweep(g, inl + e0, 0, nbits, direct, wmap, bmin, bmax, logb, runs[w]);
+    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, nbits, cnt, direct, wmap, bmin, bmax, logb, runs[w]);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -1815,16 +1928,26 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
-  // Applies mode Mode to the edge at j (v = col[j], tail blocks) of row u.
-  auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t v, uint32_t pos, uint32_t tail, bool hub,
-                  uint32_t nbv) {
+  // Applies mode Mode to the edge at j (v = col[j], tail blocks; u's row ends
+  // at CSR position re) of row u. Mode 2: a bit-row tail goes to the front of
+  // v's in-list (in_cnt[v] counts them), a column tail to the back (the first
+  // word of save[v] counts them; the savings are not needed any more).
+  auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t re, uint32_t v, uint32_t pos, uint32_t tail,
+                  bool hub, uint32_t nbv) {
     if (Mode == 0) {
       if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
     } else if (Mode == 1) {
       if (hub) atomicAdd(&in_cnt[v], 1u);
     } else if ((eflag[j >> 5] >> (j & 31)) & 1u) {
-      const uint32_t at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
-      inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
+      const uint32_t after = re - j - 1;  // u's neighbours after v
+      uint32_t at;
+      if (kHubColRatio && (uint64_t)after * 100u <= (uint64_t)tail * kHubColRatio) {
+        at = in_off[v + 1] - 1u - atomicAdd(reinterpret_cast<uint32_t*>(&save[v]), 1u);
+        inl[at] = ((uint64_t)(j + 1) << 32) | after;
+      } else {
+        at = in_off[v] + atomicAdd(&in_cnt[v], 1u);
+        inl[at] = ((uint64_t)(bs + pos) << 32) | tail;
+      }
       if (inrow) inrow[at] = u;  // timing mode only
     }
   };
@@ -1853,7 +1976,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           if (sh && (bits >> (32 - sh))) atomicOr(&eflag[(c >> 5) + 1], bits >> (32 - sh));
         }
       }
-      if (in) edge(u, bs, j, v, pos, tail, hub, nbv);
+      if (in) edge(u, bs, j, re, v, pos, tail, hub, nbv);
     }
   };
   if (Mode == 2 && u1 - u0 < 32u * nwarps) {
@@ -1893,7 +2016,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           uint32_t nbv = 0;
           const bool hub = Mode != 2 && hub_candidate<Mode>(vinfo, save, v, tail, nbv);
           if (Mode == 1 && hub) atomicOr(&eflag[j >> 5], 1u << (j & 31));
-          edge(u, bs, j, v, pos, tail, hub, nbv);
+          edge(u, bs, j, re, v, pos, tail, hub, nbv);
         }
       }
       // Longer rows: the warp, one row at a time.
@@ -1961,7 +2084,9 @@ __global__ void k_hub_total(const uint32_t* __restrict__ in_off, uint32_t n, uin
 // wave_bk[w] = the bit-row start of wave w's first row: the wave of row u is
 // the last w with wave_bk[w] <= k for any bit-row index k of u's row (a tail
 // start), so a piece's wave follows from its first tail without its row.
-__global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo, uint32_t* __restrict__ wave_bk) {
+// wave_cp[w]: the same in CSR positions, for column tails.
+__global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo, uint32_t* __restrict__ wave_bk,
+                              uint32_t* __restrict__ wave_cp) {
   const uint32_t w = threadIdx.x;
   if (w > kHubWaves) return;
   const uint64_t nb = rp_blk(g.rp[g.n]);
@@ -1976,6 +2101,7 @@ __global__ void k_wave_bounds(GraphView g, uint32_t* __restrict__ wave_lo, uint3
   }
   wave_lo[w] = w == kHubWaves ? g.n : lo;
   wave_bk[w] = w == kHubWaves ? 0xFFFFFFFFu : rp_blk(g.rp[lo]);
+  wave_cp[w] = w == kHubWaves ? 0xFFFFFFFFu : rp_row(g.rp[lo]);
 }
 
 __device__ __forceinline__ uint32_t wave_of_block(const uint32_t* __restrict__ wave_bk, uint32_t k) {
@@ -1989,13 +2115,16 @@ __device__ __forceinline__ uint32_t wave_of_block(const uint32_t* __restrict__ w
 // Counting sort of the hub pieces by the wave of their first tail, within
 // each list (CTA pieces [0, Pc), warp pieces [Pc, P)). cnt: 2 kHubWaves.
 __global__ void k_piece_waves(const uint64_t* __restrict__ pieces, const uint32_t* __restrict__ piece_off,
-                              const uint32_t* __restrict__ in_off, const uint64_t* __restrict__ inl,
-                              const uint32_t* __restrict__ wave_bk, uint32_t* __restrict__ cnt,
+                              const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_bits,
+                              const uint64_t* __restrict__ inl, const uint32_t* __restrict__ wave_bk,
+                              const uint32_t* __restrict__ wave_cp, uint32_t* __restrict__ cnt,
                               uint8_t* __restrict__ wave) {
   const uint32_t pc_n = piece_off[TRIBIT_NUM_VARIANTS + 2], all = piece_off[TRIBIT_NUM_VARIANTS + 3];
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < all; p += gridDim.x * blockDim.x) {
     const uint64_t pc = pieces[p];
-    const uint32_t w = wave_of_block(wave_bk, (uint32_t)(inl[in_off[pc >> 32] + (uint32_t)pc] >> 32));
+    const uint32_t v = (uint32_t)(pc >> 32), k = (uint32_t)pc;  // the piece's first entry: k of v's list
+    const bool bits = !kHubColRatio || k < in_bits[v];
+    const uint32_t w = wave_of_block(bits ? wave_bk : wave_cp, (uint32_t)(inl[in_off[v] + k] >> 32));
     wave[p] = (uint8_t)w;
     atomicAdd(&cnt[(p < pc_n ? 0 : kHubWaves) + w], 1u);
   }
@@ -2053,6 +2182,7 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs) {
     s.piece_wave = ar.take<uint8_t>(2 * n + E / kHubWarpPiece + 64);
     s.wave_lo = ar.take<uint32_t>(kHubWaves + 1);
     s.wave_bk = ar.take<uint32_t>(kHubWaves + 1);
+    s.wave_cp = ar.take<uint32_t>(kHubWaves + 1);
     s.wave_cnt = ar.take<uint32_t>(2 * kHubWaves);
     s.hub_pos = ar.take<uint32_t>(2 * (n + 1));
     s.hub_scan_tmp = take_scan_temp<uint32_t>(ar, 2 * (n + 1));
@@ -2083,7 +2213,8 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.in_cnt, s.in_off, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
-  k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo, s.wave_bk);
+  k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo, s.wave_bk, s.wave_cp);
+  if (kHubColRatio) TB_CUDA(cudaMemsetAsync(s.save, 0, n * sizeof(unsigned long long), st));  // column-tail counts
   TB_LAUNCH_CHECK();
   for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
     k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
@@ -2098,8 +2229,8 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   k_hub_total<<<1, 1, 0, st>>>(s.in_off, (uint32_t)n, s.piece_off);
   TB_LAUNCH_CHECK();
   TB_CUDA(cudaMemsetAsync(s.wave_cnt, 0, 2 * kHubWaves * sizeof(uint32_t), st));
-  k_piece_waves<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.in_off, s.inl, s.wave_bk, s.wave_cnt,
-                                          s.piece_wave);
+  k_piece_waves<<<148 * 8, 256, 0, st>>>(s.hub_pieces2, s.piece_off, s.in_off, s.in_cnt, s.inl, s.wave_bk,
+                                          s.wave_cp, s.wave_cnt, s.piece_wave);
   TB_LAUNCH_CHECK();
   k_wave_scan<<<1, 1, 0, st>>>(s.wave_cnt, s.piece_off);
   TB_LAUNCH_CHECK();
@@ -2198,8 +2329,8 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
   TB_LAUNCH_CHECK();
   k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
   TB_LAUNCH_CHECK();
-  k_hub<<<(unsigned)(sms * kHubCtasPerSm), kHubWarps * 32, 0, st>>>(g, s.hub_pieces, s.piece_off, s.in_off, s.inl,
-                                                                     s.inrow, stats, per_graph, cfg.block_ns);
+  k_hub<<<(unsigned)(sms * kHubCtasPerSm), kHubWarps * 32, 0, st>>>(g, s.hub_pieces, s.piece_off, s.in_off, s.in_cnt,
+                                                                     s.inl, s.inrow, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   if (cfg.variant_stop) TB_CUDA(cudaEventRecord(cfg.variant_stop, st));
   info.ctas = 2ull * warp_grid + (2ull + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? 2ull : 5ull) + kHubCtasPerSm) * sms;

@@ -64,6 +64,7 @@ struct Schedule {
   uint8_t* piece_wave = nullptr;   // device: wave of each piece's first tail
   uint32_t* wave_lo = nullptr;     // device: first row of each wave, then n
   uint32_t* wave_bk = nullptr;     // device: bit-row start of each wave's first row
+  uint32_t* wave_cp = nullptr;     // device: CSR position of each wave's first row
   uint32_t* wave_cnt = nullptr;    // device: pieces per (list, wave), scanned to positions
   uint32_t* hub_pos = nullptr;     // device, 2n + 2: piece counts, scanned to piece positions
   uint32_t* hub_scan_tmp = nullptr;

@@ -536,7 +536,7 @@ void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t
   uint64_t* keys_alt = presort ? ar.take<uint64_t>(E) : nullptr;
   RadixTemp ktmp;
   if (presort) ktmp = take_radix_temp(ar, E);
-  uint32_t* col = ar.take<uint32_t>(E ? E : 1);
+  uint32_t* col = ar.take<uint32_t>(E + 4);   // + 4: 16-byte quad loads may read three ids past the end
   uint64_t* bent = ar.take<uint64_t>(E + 2);  // + 2: 16-byte pair loads may read one entry past the end
   out->view.col = col;
   out->view.bent = bent;

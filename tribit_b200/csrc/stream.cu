@@ -366,7 +366,7 @@ size_t rows_layout(Arena& ar, bool measure, uint64_t n, uint64_t kept, uint64_t 
   ar.begin(measure);
   L->stats = ar.take<DeviceStats>(1);
   L->rp = ar.take<uint64_t>(n + 1);
-  L->col = ar.take<uint32_t>(kept ? kept : 1);
+  L->col = ar.take<uint32_t>(kept + 4);  // + 4: 16-byte quad loads may read three ids past the end
   L->bent = ar.take<uint64_t>(kept + 2);  // + 2: 16-byte pair loads may read one entry past the end
   const size_t rows_end = ar.used();
   L->row_start = ar.take<uint64_t>(n + 1);
