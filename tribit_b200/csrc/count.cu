@@ -92,6 +92,12 @@ struct BitmapProbe {
     if (blk < bmin || blk > bmax) return 0u;
     return (uint32_t)__popc((uint32_t)e & table_find(t, logb, blk));
   }
+  // Column id w (kept or not): 1 if w is in the staged row.
+  __device__ __forceinline__ uint32_t col(uint32_t w, bool keep) const {
+    const uint32_t blk = w >> 5;
+    if (!keep || blk < bmin || blk > bmax) return 0u;
+    return (table_find(t, logb, blk) >> (w & 31)) & 1u;
+  }
   // e, or an entry that matches nothing.
   static __device__ __forceinline__ uint64_t drop(uint64_t e, bool keep) { return keep ? e : 0ull; }
 };
@@ -1428,8 +1434,8 @@ __device__ __forceinline__ uint64_t sweep_col_quads(const GraphView& g, const ui
       }
 #pragma unroll
       for (int r = 0; r < DepthQuads; ++r)
-        racc += probe(col_entry(x[r].x, keep[r] & 1u)) + probe(col_entry(x[r].y, keep[r] & 2u)) +
-                probe(col_entry(x[r].z, keep[r] & 4u)) + probe(col_entry(x[r].w, keep[r] & 8u));
+        racc += probe.col(x[r].x, keep[r] & 1u) + probe.col(x[r].y, keep[r] & 2u) + probe.col(x[r].z, keep[r] & 4u) +
+                probe.col(x[r].w, keep[r] & 8u);
     }
     acc += racc;
   }
@@ -1445,6 +1451,10 @@ struct DirectProbe {
   uint32_t bmin, span;
   __device__ __forceinline__ uint32_t operator()(uint64_t e) const {
     return (uint32_t)__popc((uint32_t)e & map[min((uint32_t)(e >> 32) - bmin, span)]);
+  }
+  // Column id w: its bit of the staged mask word (a dropped id reads the zero word).
+  __device__ __forceinline__ uint32_t col(uint32_t w, bool keep) const {
+    return (map[keep ? min((w >> 5) - bmin, span) : span] >> (w & 31)) & 1u;
   }
   // e, or e with an empty mask: a dropped entry still probes, and matches nothing.
   static __device__ __forceinline__ uint64_t drop(uint64_t e, bool keep) {
