@@ -225,7 +225,8 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     c1 = tb.Counter(device=local, dispatch=dispatch)
     if dispatch == "learned":
         c1.load_model(model_path)
-    c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz)  # the batch's tuned settings
+    c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz,  # the batch's tuned settings
+                  launch_model=tb.LAUNCH_MODELS[tune.launch_model])
     idx = np.linspace(0, num_graphs - 1, per_graph_sample).astype(int)
     k_ms, e2e_one = 0.0, 0.0
     for g in idx:

@@ -179,13 +179,21 @@ typedef struct tribit_tuning {
   float merge_ratio;    /* plain dispatch: a row block not sent to the tiles goes to the sorted-list
                            merge when its neighbours' bit rows average at least merge_ratio times
                            its own rows' length, else to the bitmap sweep (default 0.75; 1e30 = never) */
+  uint32_t launch_model; /* TRIBIT_LAUNCH_KERNELS: one persistent kernel per variant;
+                            TRIBIT_LAUNCH_QUEUE: the row-piece and hub work in one persistent
+                            kernel whose CTAs take heavy rows, hub CTA pieces, then per warp
+                            bitmap, merge and hub pieces from the device cursors (the bit tiles
+                            and the fallback rows keep their kernels; ctas_per_sm unused);
+                            TRIBIT_LAUNCH_AUTO (default): the queue up to 2^24 entries, where
+                            kernel boundaries weigh most, else the kernels */
 } tribit_tuning;
+enum { TRIBIT_LAUNCH_KERNELS = 0, TRIBIT_LAUNCH_QUEUE = 1, TRIBIT_LAUNCH_AUTO = 2 };
 tribit_status tribit_get_tuning(tribit_context* ctx, tribit_tuning* out);
 /* Applies to later calls, and rebuilds the schedule of the prepared graph. */
 tribit_status tribit_set_tuning(tribit_context* ctx, const tribit_tuning* in);
 /* Times `reps` counting launches of the prepared graph for each setting of a
- * small grid (CTAs/SM x piece width x tile threshold), keeps the fastest
- * (median) and returns it. Counts stay exact under every setting. */
+ * small grid (launch model x CTAs/SM x piece width x tile threshold), keeps
+ * the fastest (median) and returns it. Counts stay exact under every setting. */
 tribit_status tribit_autotune(tribit_context* ctx, uint32_t reps, tribit_tuning* best);
 /* Arithmetic of the bit-tile variant (TRIBIT_TILES_*), for later launches;
  * rebuilds nothing, drops a captured launch. Default TRIBIT_TILES_TCGEN05. */

@@ -40,6 +40,7 @@ DISPATCH = {"plain": 0, "learned": 1, "merge": 2, "bitmap": 3, "mma": 4}
 STREAM_TIERS = {"auto": 0, "rows": 1, "pairs": 2}
 VARIANTS = ("mma", "bitmap", "merge")
 TILE_ENGINES = ("mma_sync", "tcgen05")
+LAUNCH_MODELS = ("kernels", "queue", "auto")
 
 _u64 = ctypes.c_uint64
 _u32 = ctypes.c_uint32
@@ -109,7 +110,7 @@ _decl("tribit_block_times", ctypes.c_int, _p, ctypes.c_int, _p, _u64, ctypes.POI
 class Tuning(ctypes.Structure):
     """tribit_tuning: launch parameters of the counting kernels."""
     _fields_ = [("ctas_per_sm", ctypes.c_int), ("piece_width", _u32), ("tile_min_nnz", ctypes.c_float),
-                ("count_ms", ctypes.c_float), ("merge_ratio", ctypes.c_float)]
+                ("count_ms", ctypes.c_float), ("merge_ratio", ctypes.c_float), ("launch_model", _u32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -226,11 +227,14 @@ class Counter:
         return t
 
     def set_tuning(self, ctas_per_sm: int = 0, piece_width: int = 64, tile_min_nnz: float = 64.0,
-                   merge_ratio: float | None = None):
-        """merge_ratio None keeps the context's current plain-rule merge threshold."""
+                   merge_ratio: float | None = None, launch_model: str | None = None):
+        """merge_ratio / launch_model None keep the context's current plain-rule
+        merge threshold / launch model ("kernels", "queue" or "auto")."""
+        cur = self.tuning()
         if merge_ratio is None:
-            merge_ratio = self.tuning().merge_ratio
-        t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0, merge_ratio)
+            merge_ratio = cur.merge_ratio
+        model = cur.launch_model if launch_model is None else LAUNCH_MODELS.index(launch_model)
+        t = Tuning(ctas_per_sm, piece_width, tile_min_nnz, 0.0, merge_ratio, model)
         _check(lib.tribit_set_tuning(self._h, ctypes.byref(t)), self._h)
 
     def set_tile_engine(self, engine: str):

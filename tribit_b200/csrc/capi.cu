@@ -393,15 +393,17 @@ tribit_status tribit_get_tuning(tribit_context* c, tribit_tuning* t) {
   t->tile_min_nnz = c->tile_min_nnz;
   t->count_ms = 0.f;
   t->merge_ratio = c->merge_ratio;
+  t->launch_model = c->launch_model;
   return TRIBIT_OK;
 }
 
 tribit_status tribit_set_tuning(tribit_context* c, const tribit_tuning* t) {
   if (!c || !t || t->ctas_per_sm < 0 || t->ctas_per_sm > 32 || t->piece_width < tb::kMinPieceWidth ||
       t->piece_width % 32 != 0 || t->piece_width > 4096 || !(t->tile_min_nnz >= 0.f) ||
-      !(t->merge_ratio >= 0.f))
+      !(t->merge_ratio >= 0.f) || t->launch_model > TRIBIT_LAUNCH_AUTO)
     return TRIBIT_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
+    c->launch_model = t->launch_model;
     c->ctas_per_sm = t->ctas_per_sm;
     c->piece_width = t->piece_width;
     c->tile_min_nnz = t->tile_min_nnz;
@@ -446,7 +448,7 @@ tribit_status tribit_test_tile_timeout(tribit_context* c, uint32_t max_polls) {
 tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* best) {
   if (!c || !c->prepared || !best) return TRIBIT_ERR_INVALID_ARGUMENT;
   if (reps == 0) reps = 2;
-  static const int kCtas[] = {4, 6, 7};
+  static const int kCtas[] = {4, 6, 7, 0};  // 0: the queue kernel (its CTAs per SM are fixed)
   static const uint32_t kWidths[] = {32, 64, 128};
   static const float kTile[] = {64.f, 1e30f};
   tribit_tuning cur{}, found{};
@@ -455,6 +457,7 @@ tribit_status tribit_autotune(tribit_context* c, uint32_t reps, tribit_tuning* b
   for (int ctas : kCtas)
     for (uint32_t w : kWidths)
       for (float tile : kTile) {
+        cur.launch_model = ctas ? TRIBIT_LAUNCH_KERNELS : TRIBIT_LAUNCH_QUEUE;
         cur.ctas_per_sm = ctas;
         cur.piece_width = w;
         cur.tile_min_nnz = tile;

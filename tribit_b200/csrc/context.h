@@ -53,6 +53,7 @@ struct tribit_context {
   // Device memory the context may use (tribit_set_device_budget; 0: what the
   // device has free); graphs needing more are counted in rank ranges.
   uint64_t device_budget = 0;
+  uint32_t launch_model = TRIBIT_LAUNCH_AUTO;  // tribit_tuning.launch_model
   int stream_tier = 0;                 // TRIBIT_STREAM_* (tribit_set_stream_options)
   uint64_t stream_range_entries = 0;   // bound on a rank range's entries (0: the budget's)
   tb::Arena stream_arena;              // streamed counts: degrees, ranks, row counts, piece buffers
@@ -128,6 +129,8 @@ inline CountConfig count_config(const tribit_context* c) {
   cfg.num_sms = c->num_sms;
   cfg.ctas_per_sm = c->ctas_per_sm;
   if (c->tile_wait_polls) cfg.tile_wait_polls = c->tile_wait_polls;
+  cfg.queue = c->launch_model == TRIBIT_LAUNCH_QUEUE ||
+              (c->launch_model == TRIBIT_LAUNCH_AUTO && c->prep.E <= kQueueMaxEntries);
   return cfg;
 }
 

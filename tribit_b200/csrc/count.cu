@@ -388,20 +388,32 @@ __device__ __forceinline__ unsigned long long cycles() { return (unsigned long l
 #define TB_MERGE_BITS 0
 #endif
 
+// Shared memory of the row-piece bodies: the CTA's flat table (at least
+// kWarpsPerCta * kWarpSlots words of 8 bytes, the warps' slices at `stride`
+// words apart), the warps' run buffers (`run_stride` words apart, >= 64) and
+// a CTA word.
+struct PiecesShared {
+  uint64_t* smem;
+  uint32_t stride;
+  uint32_t* runs;
+  uint32_t run_stride;
+  uint32_t* s_row;
+};
+
+// The row-piece variant V over its pieces (and, with `heavy`, first the heavy
+// rows, one CTA per row; `warp_items` false stops after them); returns this
+// thread's partial count.
 template <int V>
-__global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, const uint64_t* __restrict__ pieces,
-                                                                    const uint32_t* __restrict__ piece_off,
-                                                                    DeviceStats* stats, uint32_t* __restrict__ ovf_cta,
-                                                                    unsigned long long* per_graph,
-                                                                    unsigned long long* block_ns,
-                                                                    const uint32_t* __restrict__ heavy,
-                                                                    uint32_t width) {
-  __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
-  __shared__ uint32_t runs[kWarpsPerCta][64];
-  __shared__ uint32_t s_row;
+__device__ __forceinline__ uint64_t pieces_body(const GraphView& g, const uint64_t* __restrict__ pieces,
+                                                const uint32_t* __restrict__ piece_off, DeviceStats* stats,
+                                                uint32_t* __restrict__ ovf_cta, unsigned long long* per_graph,
+                                                unsigned long long* block_ns, const uint32_t* __restrict__ heavy,
+                                                uint32_t width, const PiecesShared& sh, bool warp_items = true) {
   constexpr bool kSorted = V == TRIBIT_VARIANT_MERGE && !TB_MERGE_BITS;  // u staged as a sorted row
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  uint64_t* tbl = smem[w];
+  uint64_t* tbl = sh.smem + w * sh.stride;
+  uint32_t* wruns = sh.runs + w * sh.run_stride;
+  uint32_t& s_row = *sh.s_row;
 
   const uint32_t p0 = piece_off[V], len = piece_off[V + 1] - p0;
   uint64_t acc = 0;
@@ -409,8 +421,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
   // time per CTA, with a CTA-shared table in the same shared memory and all
   // warps sweeping the row's neighbour chunks.
   if (heavy) {
-    uint64_t* ctbl = &smem[0][0];
-    uint32_t* pre = reinterpret_cast<uint32_t*>(&smem[kWarpsPerCta / 2][0]);
+    uint64_t* ctbl = sh.smem;
+    uint32_t* pre = reinterpret_cast<uint32_t*>(sh.smem + (kWarpsPerCta / 2) * kWarpSlots);
     const uint32_t hlen = piece_off[TRIBIT_NUM_VARIANTS + 1];
     for (;;) {
       if (threadIdx.x == 0) {
@@ -490,10 +502,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, [&](uint64_t e) -> uint32_t {
           const uint32_t o = (uint32_t)(e >> 32) - bmin;
           return o < span ? (uint32_t)__popc((uint32_t)e & cmap[o]) : 0u;
-        }, runs[w]);
+        }, wruns);
       } else {
         const BitmapProbe probe{ctbl, logb, bmin, bmax};
-        racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe, runs[w]);
+        racc = sweep_bits(g, rs + cs, rs + ce, 0, 1, probe, wruns);
       }
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
@@ -506,6 +518,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
     }
     __syncthreads();
   }
+  if (!warp_items) return acc;
   uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
   bool cur_ok = false, cur_direct = false;
   int logb = 0;
@@ -573,10 +586,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
         racc = sweep_bits(g, cs, ce, 0, 1, [&](uint64_t e) -> uint32_t {
           const uint32_t o = (uint32_t)(e >> 32) - bmin;
           return o < span ? (uint32_t)__popc((uint32_t)e & wmap[o]) : 0u;
-        }, runs[w]);
+        }, wruns);
       } else {
         const BitmapProbe probe{tbl, logb, bmin, bmax};
-        racc = sweep_bits(g, cs, ce, 0, 1, probe, runs[w]);
+        racc = sweep_bits(g, cs, ce, 0, 1, probe, wruns);
       }
       if (per_graph) {
         const uint64_t s = warp_sum(racc);
@@ -589,8 +602,24 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, 
       acc += racc;
     }
   }
+  return acc;
+}
+
+template <int V>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_pieces_warp(GraphView g, const uint64_t* __restrict__ pieces,
+                                                                    const uint32_t* __restrict__ piece_off,
+                                                                    DeviceStats* stats, uint32_t* __restrict__ ovf_cta,
+                                                                    unsigned long long* per_graph,
+                                                                    unsigned long long* block_ns,
+                                                                    const uint32_t* __restrict__ heavy,
+                                                                    uint32_t width) {
+  __shared__ __align__(16) uint64_t smem[kWarpsPerCta][kWarpSlots];
+  __shared__ uint32_t runs[kWarpsPerCta][64];
+  __shared__ uint32_t s_row;
+  const PiecesShared sh{&smem[0][0], kWarpSlots, &runs[0][0], 64, &s_row};
+  uint64_t acc = pieces_body<V>(g, pieces, piece_off, stats, ovf_cta, per_graph, block_ns, heavy, width, sh);
   acc = warp_sum(acc);
-  if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
 // ---- bit-tile MMA variant -----------------------------------------------------
@@ -1491,25 +1520,38 @@ __device__ __forceinline__ uint64_t hub_sweep_col(const GraphView& g, const uint
   return sweep_col_quads<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
 }
 
-__global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
-                                                        const uint32_t* __restrict__ piece_off,
-                                                        const uint32_t* __restrict__ in_off,
-                                                        const uint32_t* __restrict__ in_bits,
-                                                        const uint64_t* __restrict__ inl,
-                                                        const uint32_t* __restrict__ inrow, DeviceStats* stats,
-                                                        unsigned long long* per_graph,
-                                                        unsigned long long* block_ns) {
-  __shared__ __align__(16) uint32_t map[kHubMapWords];
-  __shared__ uint32_t pre[kHubPiece + 1];
-  __shared__ uint32_t runs[kHubWarps][128];
-  __shared__ uint32_t s_t;
-  __shared__ unsigned long long s_dt;
+// Shared memory of the hub body: the map (kHubMapWords words; warp w's slice
+// at w * kHubWarpStride), the tail-length prefix (kHubPiece + 1), the warps'
+// run buffers (run_stride words apart, >= 128) and two CTA words.
+struct HubShared {
+  uint32_t* map;
+  uint32_t* pre;
+  uint32_t* runs;
+  uint32_t run_stride;
+  uint32_t* s_t;
+  unsigned long long* s_dt;
+};
+
+// The hub pass: CTA pieces, then warp pieces (either part can be left out);
+// returns this thread's partial count.
+__device__ __forceinline__ uint64_t hub_body(const GraphView& g, const uint64_t* __restrict__ hub_pieces,
+                                             const uint32_t* __restrict__ piece_off,
+                                             const uint32_t* __restrict__ in_off,
+                                             const uint32_t* __restrict__ in_bits, const uint64_t* __restrict__ inl,
+                                             const uint32_t* __restrict__ inrow, DeviceStats* stats,
+                                             unsigned long long* per_graph, unsigned long long* block_ns,
+                                             const HubShared& sh, bool cta_pieces = true, bool warp_pieces = true) {
+  uint32_t* map = sh.map;
+  uint32_t* pre = sh.pre;
+  uint32_t& s_t = *sh.s_t;
+  unsigned long long& s_dt = *sh.s_dt;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* wruns = sh.runs + w * sh.run_stride;
   const uint32_t len = piece_off[TRIBIT_NUM_VARIANTS + 2];  // CTA pieces; warp pieces follow them
   const uint32_t wlen = piece_off[TRIBIT_NUM_VARIANTS + 3] - len;
   uint64_t acc = 0;
   // Phase 1: hubs with wide rows, one CTA per piece.
-  for (;;) {
+  for (; cta_pieces;) {
     if (threadIdx.x == 0) s_t = atomicAdd(&stats->cursor[kCurHub], 1u);
     __syncthreads();
     const uint32_t t = s_t;
@@ -1575,8 +1617,8 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     // Entries before nbits are bit-row tails, the rest column tails.
     const uint32_t nbits = kHubColRatio ? min(cnt, in_off[v] + in_bits[v] - min(e0, in_off[v] + in_bits[v]))
                                         : cnt;
-    uint64_t racc = hub_sweep(g, inl + e0, cs, min(ce, nbits), direct, map, bmin, bmax, logb, runs[w]);
-    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, max(cs, nbits), ce, direct, map, bmin, bmax, logb, runs[w]);
+    uint64_t racc = hub_sweep(g, inl + e0, cs, min(ce, nbits), direct, map, bmin, bmax, logb, wruns);
+    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, max(cs, nbits), ce, direct, map, bmin, bmax, logb, wruns);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -1596,7 +1638,7 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
   // Phase 2: hubs whose row fits a warp's slice of the map, one warp per
   // piece, in wave order.
   uint32_t* wmap = map + w * kHubWarpStride;
-  for (;;) {
+  for (; warp_pieces;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurHubWarp], 1u);
     const uint32_t t = __shfl_sync(kFull, t0, 0);
@@ -1628,8 +1670,8 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     __syncwarp();
     const uint32_t nbits = kHubColRatio ? min(cnt, in_off[v] + in_bits[v] - min(e0, in_off[v] + in_bits[v]))
                                         : cnt;
-    uint64_t racc = hub_sweep(g, inl + e0, 0, nbits, direct, wmap, bmin, bmax, logb, runs[w]);
-    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, nbits, cnt, direct, wmap, bmin, bmax, logb, runs[w]);
+    uint64_t racc = hub_sweep(g, inl + e0, 0, nbits, direct, wmap, bmin, bmax, logb, wruns);
+    if (kHubColRatio) racc += hub_sweep_col(g, inl + e0, nbits, cnt, direct, wmap, bmin, bmax, logb, wruns);
     if (per_graph) {
       const uint64_t s = warp_sum(racc);
       if (lane == 0 && s) atomicAdd(&per_graph[g.graph_of_rank[v]], (unsigned long long)s);
@@ -1646,8 +1688,68 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
     }
     __syncwarp();  // the slice is rewritten for the next piece
   }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphView g, const uint64_t* __restrict__ hub_pieces,
+                                                        const uint32_t* __restrict__ piece_off,
+                                                        const uint32_t* __restrict__ in_off,
+                                                        const uint32_t* __restrict__ in_bits,
+                                                        const uint64_t* __restrict__ inl,
+                                                        const uint32_t* __restrict__ inrow, DeviceStats* stats,
+                                                        unsigned long long* per_graph,
+                                                        unsigned long long* block_ns) {
+  __shared__ __align__(16) uint32_t map[kHubMapWords];
+  __shared__ uint32_t pre[kHubPiece + 1];
+  __shared__ uint32_t runs[kHubWarps][128];
+  __shared__ uint32_t s_t;
+  __shared__ unsigned long long s_dt;
+  const HubShared sh{map, pre, &runs[0][0], 128, &s_t, &s_dt};
+  uint64_t acc = hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, inrow, stats, per_graph, block_ns, sh);
   acc = warp_sum(acc);
-  if (lane == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
+}
+
+
+// ---- one persistent kernel over the work queue ------------------------------
+// The row-piece and hub work of one counting launch in one persistent kernel:
+// each CTA takes, from the device cursors in turn, heavy rows (one CTA each),
+// hub CTA pieces, then each warp bitmap pieces, merge pieces and hub warp
+// pieces, so no CTA waits at a kernel boundary for another kernel's tail. The
+// bit tiles (128-thread CTAs with tensor memory) and the fallback rows (128
+// KiB tables), which need other CTA shapes, keep their own kernels. Shared
+// memory: warp w's slice at w * kHubWarpStride words serves both bodies (a
+// row-piece table needs kWarpSlots 8-byte words), and the CTA phases use the
+// whole map.
+static_assert(kWarpsPerCta == kHubWarps, "the two bodies share the CTA shape");
+static_assert(kHubWarpStride % 4 == 0 && kHubWarpStride * 4 >= kWarpSlots * 8, "a warp slice holds a row table");
+static_assert(kHubMapWords * 4 >= kWarpsPerCta * kWarpSlots * 8, "the map holds the CTA row table and prefix");
+__global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_queue(
+    GraphView g, const uint64_t* __restrict__ pieces, const uint32_t* __restrict__ piece_off, DeviceStats* stats,
+    uint32_t* __restrict__ ovf_cta, unsigned long long* per_graph, const uint32_t* __restrict__ heavy, uint32_t width,
+    const uint64_t* __restrict__ hub_pieces, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_bits,
+    const uint64_t* __restrict__ inl) {
+  __shared__ __align__(16) uint32_t map[kHubMapWords];
+  __shared__ uint32_t pre[kHubPiece + 1];
+  __shared__ uint32_t runs[kHubWarps][128];
+  __shared__ uint32_t s_t;
+  __shared__ unsigned long long s_dt;
+  const PiecesShared ps{reinterpret_cast<uint64_t*>(map), kHubWarpStride / 2, &runs[0][0], 128, &s_t};
+  const HubShared hs{map, pre, &runs[0][0], 128, &s_t, &s_dt};
+  uint64_t acc = 0;
+  // CTA phases (each ends with all of the CTA's threads past a barrier):
+  // heavy rows, then the hub's CTA pieces.
+  acc += pieces_body<TRIBIT_VARIANT_BITMAP>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, heavy, width, ps,
+                                            false);
+  acc += hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, nullptr, stats, per_graph, nullptr, hs, true, false);
+  // Warp phases, each warp in its own slice: bitmap, merge and hub warp pieces.
+  acc += pieces_body<TRIBIT_VARIANT_BITMAP>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, nullptr, width,
+                                            ps);
+  acc += pieces_body<TRIBIT_VARIANT_MERGE>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, nullptr, width,
+                                           ps);
+  acc += hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, nullptr, stats, per_graph, nullptr, hs, false, true);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
 
 // ---- schedule ----------------------------------------------------------------
@@ -2316,6 +2418,30 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
   TB_CUDA(cudaMemsetAsync(&stats->triangles, 0, sizeof(stats->triangles), st));
   uint32_t* ovf_cta = s.overflow;
   uint32_t* ovf_global = s.overflow + s.overflow_cap;
+  if (cfg.queue && !cfg.block_ns && !cfg.variant_start) {
+    // One persistent kernel for the row pieces and the hub pass; the tiles and
+    // the fallback rows (whose list k_queue fills) after it.
+    k_queue<<<(unsigned)(sms * kHubCtasPerSm), kHubWarps * 32, 0, st>>>(
+        g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, s.heavy, s.piece_width, s.hub_pieces, s.in_off,
+        s.in_cnt, s.inl);
+    TB_LAUNCH_CHECK();
+    if (s.tile_engine == TRIBIT_TILES_TCGEN05)
+      k_tiles_tc<<<(unsigned)(sms * 2), kTcThreads, sizeof(TcSmem), st>>>(g, s.pieces, s.piece_off, stats, per_graph,
+                                                                           nullptr, cfg.tile_wait_polls,
+                                                                           cfg.tile_test_no_commit);
+    else
+      k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
+          g, s.pieces, s.piece_off, stats, per_graph, nullptr);
+    TB_LAUNCH_CHECK();
+    k_rows_cta<<<(unsigned)sms, kCtaThreads, sizeof(uint64_t) << kCtaLogSlots, st>>>(g, ovf_cta, stats, ovf_global,
+                                                                                     per_graph, nullptr);
+    TB_LAUNCH_CHECK();
+    k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
+    TB_LAUNCH_CHECK();
+    info.ctas = (uint64_t)(kHubCtasPerSm + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? 2 : 5) + 2) * sms;
+    info.kernels = 4;
+    return info;
+  }
   // Timing mode: the events bracket every counting kernel, and every piece,
   // heavy row, tile block and hub piece adds its warp-cycles to its row block.
   if (cfg.variant_start) TB_CUDA(cudaEventRecord(cfg.variant_start, st));

@@ -87,7 +87,14 @@ struct CountConfig {
   cudaEvent_t variant_stop = nullptr;      // all counting kernels
   uint32_t tile_wait_polls = 1u << 22;     // tcgen05 tiles: mbarrier polls before a wait gives up
   int tile_test_no_commit = 0;             // failure-detection test: tile MMAs never committed
+  bool queue = false;                      // TRIBIT_LAUNCH_QUEUE (not in the timing mode)
 };
+
+// TRIBIT_LAUNCH_AUTO takes the queue kernel up to this many entries: on one
+// B200 it counted Chung-Lu n = 7,115 in 0.051 ms instead of 0.085, RMAT-16
+// 32% and RMAT-18 12% faster, RMAT-20 (2^24 entries) even, and RMAT-21 to 24
+// 3-5% slower (5 CTAs an SM for the row pieces instead of 6-7).
+constexpr uint64_t kQueueMaxEntries = 1ull << 24;
 
 // hubs: also take the hub-pass arrays (about 13 bytes per entry).
 Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs = true);

@@ -119,6 +119,7 @@ extern "C" tribit_status tribit_count_edges_noalloc(const uint64_t* d_entries, u
     tb::build_schedule(prep.view, sched, TRIBIT_DISPATCH_PLAIN, hubs, st);
     tb::CountConfig cfg;
     cfg.num_sms = sms;
+    cfg.queue = true;  // graphs that fit the scratch are small: one queue-driven kernel
     tb::launch_count(prep.view, sched, prep.stats, nullptr, cfg, st);
     k_noalloc_result<<<1, 1, 0, st>>>(prep.stats, hubs, reinterpret_cast<unsigned long long*>(d_result));
     TB_LAUNCH_CHECK();
