@@ -401,14 +401,13 @@ struct PiecesShared {
 };
 
 // The row-piece variant V over its pieces (and, with `heavy`, first the heavy
-// rows, one CTA per row; `warp_items` false stops after them); returns this
-// thread's partial count.
+// rows, one CTA per row); returns this thread's partial count.
 template <int V>
 __device__ __forceinline__ uint64_t pieces_body(const GraphView& g, const uint64_t* __restrict__ pieces,
                                                 const uint32_t* __restrict__ piece_off, DeviceStats* stats,
                                                 uint32_t* __restrict__ ovf_cta, unsigned long long* per_graph,
                                                 unsigned long long* block_ns, const uint32_t* __restrict__ heavy,
-                                                uint32_t width, const PiecesShared& sh, bool warp_items = true) {
+                                                uint32_t width, const PiecesShared& sh) {
   constexpr bool kSorted = V == TRIBIT_VARIANT_MERGE && !TB_MERGE_BITS;  // u staged as a sorted row
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* tbl = sh.smem + w * sh.stride;
@@ -518,7 +517,6 @@ __device__ __forceinline__ uint64_t pieces_body(const GraphView& g, const uint64
     }
     __syncthreads();
   }
-  if (!warp_items) return acc;
   uint32_t cur = 0xFFFFFFFFu;  // row whose structure is loaded
   bool cur_ok = false, cur_direct = false;
   int logb = 0;
@@ -1532,15 +1530,14 @@ struct HubShared {
   unsigned long long* s_dt;
 };
 
-// The hub pass: CTA pieces, then warp pieces (either part can be left out);
-// returns this thread's partial count.
+// The hub pass: CTA pieces, then warp pieces; returns this thread's partial count.
 __device__ __forceinline__ uint64_t hub_body(const GraphView& g, const uint64_t* __restrict__ hub_pieces,
                                              const uint32_t* __restrict__ piece_off,
                                              const uint32_t* __restrict__ in_off,
                                              const uint32_t* __restrict__ in_bits, const uint64_t* __restrict__ inl,
                                              const uint32_t* __restrict__ inrow, DeviceStats* stats,
                                              unsigned long long* per_graph, unsigned long long* block_ns,
-                                             const HubShared& sh, bool cta_pieces = true, bool warp_pieces = true) {
+                                             const HubShared& sh) {
   uint32_t* map = sh.map;
   uint32_t* pre = sh.pre;
   uint32_t& s_t = *sh.s_t;
@@ -1551,7 +1548,7 @@ __device__ __forceinline__ uint64_t hub_body(const GraphView& g, const uint64_t*
   const uint32_t wlen = piece_off[TRIBIT_NUM_VARIANTS + 3] - len;
   uint64_t acc = 0;
   // Phase 1: hubs with wide rows, one CTA per piece.
-  for (; cta_pieces;) {
+  for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(&stats->cursor[kCurHub], 1u);
     __syncthreads();
     const uint32_t t = s_t;
@@ -1638,7 +1635,7 @@ __device__ __forceinline__ uint64_t hub_body(const GraphView& g, const uint64_t*
   // Phase 2: hubs whose row fits a warp's slice of the map, one warp per
   // piece, in wave order.
   uint32_t* wmap = map + w * kHubWarpStride;
-  for (; warp_pieces;) {
+  for (;;) {
     uint32_t t0 = 0;
     if (lane == 0) t0 = atomicAdd(&stats->cursor[kCurHubWarp], 1u);
     const uint32_t t = __shfl_sync(kFull, t0, 0);
@@ -1714,8 +1711,9 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_hub(GraphVi
 // ---- one persistent kernel over the work queue ------------------------------
 // The row-piece and hub work of one counting launch in one persistent kernel:
 // each CTA takes, from the device cursors in turn, heavy rows (one CTA each),
-// hub CTA pieces, then each warp bitmap pieces, merge pieces and hub warp
-// pieces, so no CTA waits at a kernel boundary for another kernel's tail. The
+// then each warp bitmap and merge pieces, then the CTA hub CTA pieces and each
+// warp hub warp pieces, so no CTA waits at a kernel boundary for another
+// kernel's tail. The
 // bit tiles (128-thread CTAs with tensor memory) and the fallback rows (128
 // KiB tables), which need other CTA shapes, keep their own kernels. Shared
 // memory: warp w's slice at w * kHubWarpStride words serves both bodies (a
@@ -1737,17 +1735,15 @@ __global__ void __launch_bounds__(kHubWarps * 32, TB_HUB_MIN_CTAS) k_queue(
   const PiecesShared ps{reinterpret_cast<uint64_t*>(map), kHubWarpStride / 2, &runs[0][0], 128, &s_t};
   const HubShared hs{map, pre, &runs[0][0], 128, &s_t, &s_dt};
   uint64_t acc = 0;
-  // CTA phases (each ends with all of the CTA's threads past a barrier):
-  // heavy rows, then the hub's CTA pieces.
-  acc += pieces_body<TRIBIT_VARIANT_BITMAP>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, heavy, width, ps,
-                                            false);
-  acc += hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, nullptr, stats, per_graph, nullptr, hs, true, false);
-  // Warp phases, each warp in its own slice: bitmap, merge and hub warp pieces.
-  acc += pieces_body<TRIBIT_VARIANT_BITMAP>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, nullptr, width,
-                                            ps);
+  // The separate kernels' order: heavy rows (CTA), bitmap and merge pieces
+  // (warps), then, once the CTA's warps meet, the hub's CTA pieces and its
+  // warp pieces. (Hub CTA pieces right after the heavy rows, before the warp
+  // pieces, measured 0.5-3% slower on RMAT-18 to 24.)
+  acc += pieces_body<TRIBIT_VARIANT_BITMAP>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, heavy, width, ps);
   acc += pieces_body<TRIBIT_VARIANT_MERGE>(g, pieces, piece_off, stats, ovf_cta, per_graph, nullptr, nullptr, width,
                                            ps);
-  acc += hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, nullptr, stats, per_graph, nullptr, hs, false, true);
+  __syncthreads();  // the hub's CTA pieces take the whole map
+  acc += hub_body(g, hub_pieces, piece_off, in_off, in_bits, inl, nullptr, stats, per_graph, nullptr, hs);
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&stats->triangles, (unsigned long long)acc);
 }
