@@ -1283,6 +1283,9 @@ constexpr uint32_t kHubWarpPiece = TB_HUB_WARP_PIECE;  // in-edges per warp piec
 #define TB_HUB_WAVES 32
 #endif
 constexpr uint32_t kHubWaves = TB_HUB_WAVES;    // row ranges the hub pieces are ordered by (power of 2)
+// Up to this many entries (bit rows of at most 64 MiB) the in-lists are filled
+// in one launch instead of one per wave.
+constexpr uint64_t kHubOneWaveEntries = 1ull << 23;
 // Five CTAs per SM (48 registers), the occupancy the 41 KiB of shared memory
 // allows; with four the pair loads' extra registers cost more than they save.
 #ifndef TB_HUB_MIN_CTAS
@@ -2324,10 +2327,18 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo, s.wave_bk, s.wave_cp);
   if (kHubColRatio) TB_CUDA(cudaMemsetAsync(s.save, 0, n * sizeof(unsigned long long), st));  // column-tail counts
   TB_LAUNCH_CHECK();
-  for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
+  if (s.inl_cap <= kHubOneWaveEntries) {
+    // A graph whose bit rows fit the L2 many times over gains nothing from
+    // the wave order: one launch fills every in-list.
     k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                             s.hub_rows ? s.inrow : nullptr, s.wave_lo + w);
+                                             s.hub_rows ? s.inrow : nullptr, nullptr);
     TB_LAUNCH_CHECK();
+  } else {
+    for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
+      k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+                                               s.hub_rows ? s.inrow : nullptr, s.wave_lo + w);
+      TB_LAUNCH_CHECK();
+    }
   }
   k_hub_piece_count<<<vblocks, 256, 0, st>>>(s.in_off, s.vinfo, (uint32_t)n, s.hub_pos);
   TB_LAUNCH_CHECK();
