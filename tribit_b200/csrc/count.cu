@@ -1306,6 +1306,10 @@ constexpr bool kHubPairs = TB_HUB_PAIRS != 0;   // tails read as 16-byte pairs o
 #define TB_HUB_COL_RATIO 175
 #endif
 constexpr uint32_t kHubColRatio = TB_HUB_COL_RATIO;
+#ifndef TB_HUB_COL_DEPTH
+#define TB_HUB_COL_DEPTH 2
+#endif
+constexpr int kHubColDepth = TB_HUB_COL_DEPTH;  // 16-byte quads of column ids in flight per lane
 
 // Walks the tails of in-list entries [cs, ce) (at list) against v's staged row:
 // direct-mapped masks over blocks [bmin, bmin + span) in map, or a bucketed
@@ -1516,9 +1520,9 @@ __device__ __forceinline__ uint64_t hub_sweep_col(const GraphView& g, const uint
                                                   uint32_t ce, bool direct, const uint32_t* map, uint32_t bmin,
                                                   uint32_t bmax, int logb, uint32_t* wsm) {
   if (cs >= ce) return 0;  // uniform across the warp
-  if (direct) return sweep_col_quads<kHubDepth / 2>(g, list, cs, ce, DirectProbe{map, bmin, bmax - bmin + 1}, wsm);
+  if (direct) return sweep_col_quads<kHubColDepth>(g, list, cs, ce, DirectProbe{map, bmin, bmax - bmin + 1}, wsm);
   const BitmapProbe probe{reinterpret_cast<const uint64_t*>(map), logb, bmin, bmax};
-  return sweep_col_quads<kHubDepth / 2>(g, list, cs, ce, probe, wsm);
+  return sweep_col_quads<kHubColDepth>(g, list, cs, ce, probe, wsm);
 }
 
 // Shared memory of the hub body: the map (kHubMapWords words; warp w's slice
