@@ -56,10 +56,12 @@ def test_streamed_counts_match_oracle(name, n, make):
             assert r.stream_tier in (ROWS, PAIRS)
             if r.stream_tier == ROWS:
                 # The rows tier builds the one-piece oriented graph, range by
-                # range; a small budget may leave no room for the hub in-lists
-                # (the merge blocks then count without the hub pass).
-                assert r.stream_tasks == 1 and _schedule(r)[:2] == one_piece[:2], (name, frac)
-                assert r.hub_edges in (0, one_piece[2]) and (frac < 0.8 or r.hub_edges == one_piece[2]), (name, frac)
+                # range; a small budget may leave no room for the hub in-lists,
+                # and the dispatcher's merge blocks then go to the bitmap sweep.
+                assert r.stream_tasks == 1 and r.row_blocks == one_piece[0], (name, frac)
+                mma, bitmap, merge = one_piece[1]
+                assert _schedule(r) == one_piece or (r.hub_edges == 0 and frac < 0.8 and
+                                                     _schedule(r)[1] == (mma, bitmap + merge, 0)), (name, frac)
         # Rows tier in a few ranges (filled from the streamed entries) and in
         # many (from host buckets): the same graph again.
         c.set_device_budget(int(need * 0.8))

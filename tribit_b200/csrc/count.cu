@@ -2401,6 +2401,20 @@ void compute_features(const GraphView& g, Schedule& s, int mode, bool full_featu
   TB_LAUNCH_CHECK();
 }
 
+namespace {
+__global__ void k_merge_to_bitmap(uint8_t* __restrict__ variant_of, uint32_t nrb) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nrb; i += gridDim.x * blockDim.x)
+    if (variant_of[i] == TRIBIT_VARIANT_MERGE) variant_of[i] = TRIBIT_VARIANT_BITMAP;
+}
+}  // namespace
+
+void merge_blocks_to_bitmap(Schedule& s, cudaStream_t st) {
+  if (s.num_row_blocks == 0) return;
+  k_merge_to_bitmap<<<(unsigned)ceil_div<uint64_t>(s.num_row_blocks, 256), 256, 0, st>>>(s.variant_of,
+                                                                                         s.num_row_blocks);
+  TB_LAUNCH_CHECK();
+}
+
 void build_schedule(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st) {
   compute_features(g, s, mode, full_features, st);
   build_pieces(g, s, st);

@@ -102,6 +102,8 @@ Schedule take_schedule(Arena& ar, uint64_t n, uint64_t E, bool hubs = true);
 // Computes row-block features, the per-block variant (mode: TRIBIT_DISPATCH_*),
 // and the per-variant piece lists. full_features adds the neighbour-side
 // features (one extra pass over the edges) the learned dispatcher needs.
+// Sends the row blocks dispatched to the merge variant to the bitmap sweep.
+void merge_blocks_to_bitmap(Schedule& s, cudaStream_t st);
 void build_schedule(const GraphView& g, Schedule& s, int mode, bool full_features, cudaStream_t st);
 
 // Row-block features (full adds the neighbour-side ones) and the plain or

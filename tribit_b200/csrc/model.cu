@@ -351,10 +351,16 @@ void apply_dispatch(tribit_context* c, cudaStream_t st) {
     require_model(c);
     compute_features(c->prep.view, c->sched, TRIBIT_DISPATCH_PLAIN, true, st);
     model_dispatch(c->model, c->sched.features, c->sched.num_row_blocks, c->sched.variant_of, st);
-    build_pieces(c->prep.view, c->sched, st);
   } else {
-    build_schedule(c->prep.view, c->sched, mode, mode == TRIBIT_DISPATCH_PLAIN, st);
+    compute_features(c->prep.view, c->sched, mode, mode == TRIBIT_DISPATCH_PLAIN, st);
   }
+  // Both rules choose merge for the hub pass; a schedule taken without hub
+  // lists (the rows tier under a small device budget) sweeps those blocks as
+  // bitmaps instead (RMAT-24: 132 ms all-bitmap against 168 ms merge without
+  // the hub pass).
+  if (!c->sched.eflag && (mode == TRIBIT_DISPATCH_LEARNED || mode == TRIBIT_DISPATCH_PLAIN))
+    merge_blocks_to_bitmap(c->sched, st);
+  build_pieces(c->prep.view, c->sched, st);
 }
 
 }  // namespace tb
