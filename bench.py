@@ -500,6 +500,8 @@ def main():
                 "budget_gb": round(need * frac / 1e9, 3), "one_piece_gb": round(need / 1e9, 3),
                 "tier": ("one piece", "rows", "pairs")[last.stream_tier], "ranges": last.stream_ranges,
                 "tasks": last.stream_tasks, "value": job_edges / t, "ms_per_step": t * 1e3,
+                # host wall times of the call's uploads and of the rest before counting
+                "h2d_ms": last.h2d_ms, "preprocess_ms": last.preprocess_ms,
                 "count_ms": last.kernel_ms, "hub_edges": last.hub_edges}
 
     streamed = [streamed_run(f.strip()) for f in args.stream_budgets.split(",") if f.strip()]
