@@ -243,6 +243,7 @@ void tribit_destroy(tribit_context* c) {
     c->load_arena.release();
     for (auto& p : c->pinned)
       if (p) cudaFreeHost(p);
+    if (c->stream_host) cudaFreeHost(c->stream_host);
     tb::drop_graph(c);
     c->train_arena.release();
     c->timing_arena.release();

@@ -57,6 +57,8 @@ struct tribit_context {
   int stream_tier = 0;                 // TRIBIT_STREAM_* (tribit_set_stream_options)
   uint64_t stream_range_entries = 0;   // bound on a rank range's entries (0: the budget's)
   tb::Arena stream_arena;              // streamed counts: degrees, ranks, row counts, piece buffers
+  void* stream_host = nullptr;         // streamed counts: pinned host row starts and ranks (kept)
+  size_t stream_host_bytes = 0;
   tb::Arena train_arena;               // training batches and activations
   tb::Arena timing_arena;              // per-row-block cycle counters
   std::string err;

@@ -416,16 +416,51 @@ bool plan_rows(Arena& ar, uint64_t n, uint64_t kept, uint32_t max_row, uint64_t 
 struct RowsSource {
   const std::vector<std::unique_ptr<uint64_t[]>>* bucket = nullptr;  // null: streamed
   const PieceStream* stream = nullptr;
-  const std::vector<uint32_t>* rank = nullptr;  // streamed: the rank of every vertex
 };
+
+// Host copies of phase 1's row starts (n + 1) and ranks (n) for phase 2: the
+// context's pinned buffer, kept for later calls (copied straight both ways),
+// or pageable memory when that cannot be had.
+struct CarryHost {
+  uint64_t* off = nullptr;
+  uint32_t* rank = nullptr;
+  bool pinned = false;
+  std::vector<uint64_t> off_v;
+  std::vector<uint32_t> rank_v;
+};
+
+void carry_host(tribit_context* c, uint64_t n, CarryHost* h) {
+  const size_t bytes = (n + 1) * sizeof(uint64_t) + n * sizeof(uint32_t);
+  if (c->stream_host_bytes < bytes) {
+    if (c->stream_host) cudaFreeHost(c->stream_host);
+    c->stream_host = nullptr;
+    c->stream_host_bytes = 0;
+    if (cudaMallocHost(&c->stream_host, bytes) == cudaSuccess) {
+      c->stream_host_bytes = bytes;
+    } else {
+      (void)cudaGetLastError();
+      c->stream_host = nullptr;
+    }
+  }
+  if (c->stream_host) {
+    h->off = static_cast<uint64_t*>(c->stream_host);
+    h->rank = reinterpret_cast<uint32_t*>(h->off + n + 1);
+    h->pinned = true;
+  } else {
+    h->off_v.resize(n + 1);
+    h->rank_v.resize(n);
+    h->off = h->off_v.data();
+    h->rank = h->rank_v.data();
+  }
+}
 
 // Phase 2 of the rows tier: each range's rows built in rank order into one
 // resident oriented graph, which the context then holds prepared (as a
 // one-piece count leaves it) and counts once. size[r]: range r's entries.
 void count_rows_tier(tribit_context* c, const RowsSource& src, const std::vector<uint64_t>& size,
-                     const std::vector<uint32_t>& hb, const std::vector<uint64_t>& h_off, uint64_t n, uint64_t E,
-                     uint64_t kept, bool hubs, uint64_t cap, uint64_t piece_words,
-                     std::chrono::steady_clock::time_point t0, tribit_result* res) {
+                     const std::vector<uint32_t>& hb, const CarryHost& carry, uint64_t n, uint64_t E, uint64_t kept,
+                     bool hubs, uint64_t cap, uint64_t piece_words, std::chrono::steady_clock::time_point t0,
+                     tribit_result* res) {
   cudaStream_t st = c->st;
   Arena& ar = c->arena;
   RowsLayout L;
@@ -438,10 +473,14 @@ void count_rows_tier(tribit_context* c, const RowsSource& src, const std::vector
     upload_via_pinned(c, from, bytes, dst);
     h2d_ms += ms_since(tu);
   };
-  upload(h_off.data(), (n + 1) * sizeof(uint64_t), L.row_start);
+  auto upload_carry = [&](const void* from, size_t bytes, void* dst) {
+    if (!carry.pinned) return upload(from, bytes, dst);
+    TB_CUDA(cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, st));
+  };
+  upload_carry(carry.off, (n + 1) * sizeof(uint64_t), L.row_start);
   PieceStream ps;
   if (!src.bucket) {
-    upload(src.rank->data(), n * sizeof(uint32_t), L.rank);
+    upload_carry(carry.rank, n * sizeof(uint32_t), L.rank);
     ps = *src.stream;
     ps.pieces[0] = L.pieces[0];
     ps.pieces[1] = L.pieces[1];
@@ -521,7 +560,10 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
     throw StatusError(TRIBIT_ERR_TOO_LARGE, "counting in rank ranges takes fewer than 2^31 vertices");
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = c->st;
-  c->arena.release();  // the in-core layout does not fit: its reservation goes to the pieces
+  // Phase 1 and the rows tier run in the context's arena, kept across calls of
+  // the same budget (no reallocation); the pairs tier's buffer in its own.
+  if (c->arena.capacity() > budget) c->arena.release();
+  c->stream_arena.release();
   drop_graph(c);
   c->prepared = false;
 
@@ -530,7 +572,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   // entries (phase 1's piece buffers take 36 bytes an entry: two piece
   // buffers, keys, ranges, grouped keys; the rows tier's two take 16).
   const uint64_t piece_words = std::max<uint64_t>(1u << 14, std::min<uint64_t>(kPieceWords, budget / 2048));
-  Arena& ar = c->stream_arena;
+  Arena& ar = c->arena;
   uint32_t *deg = nullptr, *rank = nullptr, *rows = nullptr, *bounds = nullptr, *hist = nullptr, *rng = nullptr;
   uint64_t *off = nullptr, *otmp = nullptr, *size = nullptr, *keys = nullptr, *part = nullptr;
   uint64_t* pieces[2] = {nullptr, nullptr};
@@ -639,18 +681,18 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   // it fills each one straight from the entries streamed again (the ranks
   // orient them), instead of sending every key to a host bucket and back.
   const bool direct = rows_tier && P <= (ps.pinned_src ? kDirectRangesPinned : kDirectRangesPageable);
-  std::vector<uint64_t> h_off(rows_tier ? n + 1 : 0);
-  std::vector<uint32_t> h_rank(direct ? n : 0);
-  if (rows_tier) TB_CUDA(cudaMemcpyAsync(h_off.data(), off, (n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  if (direct) TB_CUDA(cudaMemcpyAsync(h_rank.data(), rank, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CarryHost carry;
+  if (rows_tier) {
+    carry_host(c, n, &carry);
+    TB_CUDA(cudaMemcpyAsync(carry.off, off, (n + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  }
+  if (direct) TB_CUDA(cudaMemcpyAsync(carry.rank, rank, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   TB_CUDA(cudaStreamSynchronize(st));
 
-  if (direct) {
-    ar.release();  // phase 1 is done: its device memory goes to phase 2
+  if (direct) {  // phase 1 is done: the arena's space goes to phase 2
     RowsSource src;
     src.stream = &ps;
-    src.rank = &h_rank;
-    count_rows_tier(c, src, hsize, hb, h_off, n, E, kept, plan.hubs, cap, piece_words, t0, res);
+    count_rows_tier(c, src, hsize, hb, carry, n, E, kept, plan.hubs, cap, piece_words, t0, res);
     if (res) res->stream_ranges = (uint32_t)P;
     return true;
   }
@@ -687,18 +729,19 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   check_flags(nullptr);
   for (uint64_t r = 0; r < P; ++r)
     if (filled[r] != hsize[r]) throw StatusError(TRIBIT_ERR_INVALID_ARGUMENT, "the host entries changed during the count");
-  ar.release();  // phase 1 is done: its device memory goes to phase 2
   const float phase1_ms = ms_since(t0);
 
   if (rows_tier) {
     RowsSource src;
     src.bucket = &bucket;
-    count_rows_tier(c, src, hsize, hb, h_off, n, E, kept, plan.hubs, cap, piece_words, t0, res);
+    count_rows_tier(c, src, hsize, hb, carry, n, E, kept, plan.hubs, cap, piece_words, t0, res);
     if (res) res->stream_ranges = (uint32_t)P;
     return true;
   }
 
   // ---- phase 2 of the pairs tier: every pair of ranges i <= j ------------------
+  ar.release();  // the tasks size the context's arena themselves
+  Arena& wa = c->stream_arena;
   uint64_t tri = 0, edges = 0, ctas = 0, blocks = 0, tasks = 0;
   uint64_t by_variant[TRIBIT_NUM_VARIANTS] = {0, 0, 0};
   float prep_ms = 0.f, kernel_ms = 0.f, h2d_ms = 0.f;
@@ -708,10 +751,10 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   for (uint64_t r = 0; r < P; ++r) max_bucket = std::max(max_bucket, filled[r]);
   uint64_t* w = nullptr;
   for (int pass = 0; pass < 2; ++pass) {
-    ar.begin(pass == 0);
-    w = ar.take<uint64_t>(3 * max_bucket + 1);
-    extra = ar.take<unsigned long long>(1);
-    if (pass == 0) ar.reserve(ar.used(), false);
+    wa.begin(pass == 0);
+    w = wa.take<uint64_t>(3 * max_bucket + 1);
+    extra = wa.take<unsigned long long>(1);
+    if (pass == 0) wa.reserve(wa.used(), false);
   }
   for (uint64_t i = 0; i < P; ++i) {
     for (uint64_t j = i; j < P; ++j) {
@@ -756,6 +799,7 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
   // The tasks' graphs are not the input graph: the context keeps nothing prepared.
   c->prepared = false;
   drop_graph(c);
+  wa.release();
   if (res) {
     std::memset(res, 0, sizeof *res);
     res->triangles = tri;
