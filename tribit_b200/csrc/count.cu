@@ -1997,40 +1997,38 @@ __global__ void k_hub_vinfo(GraphView g, uint64_t* __restrict__ vinfo) {
   vinfo[v] = x;
 }
 
-// Hub decision for the edge at CSR position j (u -> v, v's block at index pos
-// of u's bit row of nbu entries): the tail of u is shorter than v's row and v
-// can be staged; in mode 1 also v saves at least its staging cost (the direct
-// map's span / 4 vector stores, or a hash's 2 nb slots cleared, plus nb inserts).
-// Mode 0 adds a candidate's saving only while save[v] is below that cost: the
-// decision save[v] >= cost is then the one the full sum gives (an add is
-// skipped only when the sum has already reached the cost), without one
-// atomic per in-edge on the most popular hubs.
+// Hub candidate: the edge at CSR position j (u -> v; v's block at index pos of
+// u's bit row, u's tail `tail` blocks from it) whose tail is shorter than v's
+// row, with v stageable. cost: what staging v's row costs (the direct map's
+// span / 4 vector stores, or a hash's 2 nb slots cleared, plus nb inserts).
 __device__ __forceinline__ unsigned long long hub_cost(uint32_t span, uint32_t nbv) {
   return span <= kHubMaxSpan ? (unsigned long long)(span / 4 + nbv)
                              : (unsigned long long)kHubHashMul * 3ull * nbv + kHubHashMin;
 }
 
-template <int Mode>
-__device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo,
-                                              const unsigned long long* __restrict__ save, uint32_t v,
-                                              uint32_t tail, uint32_t& nbv) {
+__device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo, uint32_t v, uint32_t tail,
+                                              uint32_t& nbv, unsigned long long& cost) {
   const uint64_t vi = vinfo[v];
   nbv = (uint32_t)vi;
   const uint32_t span = (uint32_t)(vi >> 32);
-  bool hub = nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
-  if (Mode == 1) hub = hub && save[v] >= hub_cost(span, nbv);
-  if (Mode == 0) hub = hub && *(volatile const unsigned long long*)&save[v] < hub_cost(span, nbv);
-  return hub;
+  cost = hub_cost(span, nbv);
+  return nbv > 0 && tail < nbv && (span <= kHubMaxSpan || (kHubHashMul > 0 && nbv <= kHubMaxHash));
 }
 
-// One pass over the edges of the merge row blocks. Modes 0 and 1: one warp
-// per row block; rows of at most kHubLaneRow neighbours are walked by their
-// own lane, longer rows by the whole warp. Mode 2: one warp per row. For the edge at CSR position j, u's tail is u's bit
-// blocks from v's block on. Mode 0: save[v] += the blocks a hub walk saves
-// (v's row length - tail) over the candidate edges. Mode 1: flags the edges
-// whose hub saves at least its staging cost and counts them per hub. Mode 2:
-// appends each flagged edge's tail (first block, length) and row to its hub's
-// in-list. rows (may be null): the pass covers rows [rows[0], rows[1]).
+// One pass over the edges of the merge row blocks; rows of at most
+// kHubLaneRow neighbours are walked by their own lane, longer rows by the
+// whole warp (mode 1 on a small wave: one warp per row). For the edge at CSR
+// position j, u's tail is u's bit blocks from v's block on.
+// Mode 0: counts each hub's candidate in-edges (in_cnt) and adds to save[v]
+// the blocks a hub walk saves (v's row length - tail), but only while save[v]
+// is below the staging cost: the decision save[v] >= cost (k_hub_accept) is
+// then the one the full sum gives, without one atomic per in-edge on the
+// most popular hubs.
+// Mode 1: every candidate edge of an accepted hub (save[v] >> 32 set) is
+// flagged and appended to the hub's in-list: a bit-row tail (first block,
+// blocks) at the front (in_cnt[v] counts them), a column tail (first CSR
+// position after v, neighbours) at the back (the low word of save[v] counts
+// them). rows (may be null): the pass covers rows [rows[0], rows[1]).
 constexpr uint32_t kHubLaneRow = 64;
 
 template <int Mode>
@@ -2043,17 +2041,21 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
-  // Applies mode Mode to the edge at j (v = col[j], tail blocks; u's row ends
-  // at CSR position re) of row u. Mode 2: a bit-row tail goes to the front of
-  // v's in-list (in_cnt[v] counts them), a column tail to the back (the first
-  // word of save[v] counts them; the savings are not needed any more).
+  // Whether the edge to v (tail blocks) takes part: mode 0, a candidate;
+  // mode 1, a candidate of an accepted hub.
+  auto decide = [&](uint32_t v, uint32_t tail, uint32_t& nbv, unsigned long long& cost) -> bool {
+    const bool cand = hub_candidate(vinfo, v, tail, nbv, cost);
+    if (Mode == 0) return cand;
+    return cand && (save[v] >> 32) != 0;
+  };
+  // Applies mode Mode to the taking-part edge at j (v = col[j]; u's row ends
+  // at CSR position re) of row u.
   auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t re, uint32_t v, uint32_t pos, uint32_t tail,
-                  bool hub, uint32_t nbv) {
+                  uint32_t nbv, unsigned long long cost) {
     if (Mode == 0) {
-      if (hub) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
-    } else if (Mode == 1) {
-      if (hub) atomicAdd(&in_cnt[v], 1u);
-    } else if ((eflag[j >> 5] >> (j & 31)) & 1u) {
+      atomicAdd(&in_cnt[v], 1u);
+      if (*(volatile const unsigned long long*)&save[v] < cost) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
+    } else {
       const uint32_t after = re - j - 1;  // u's neighbours after v
       uint32_t at;
       if (kHubColRatio && (uint64_t)after * 100u <= (uint64_t)tail * kHubColRatio) {
@@ -2082,7 +2084,8 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
       prev_last = __shfl_sync(kFull, blk, 31);
       const uint32_t tail = nb - pos;
       uint32_t nbv = 0;
-      const bool hub = in && Mode != 2 && hub_candidate<Mode>(vinfo, save, v, tail, nbv);
+      unsigned long long cost = 0;
+      const bool hub = in && decide(v, tail, nbv, cost);
       if (Mode == 1) {
         const uint32_t bits = __ballot_sync(kFull, hub);
         if (lane == 0 && bits) {
@@ -2091,10 +2094,10 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           if (sh && (bits >> (32 - sh))) atomicOr(&eflag[(c >> 5) + 1], bits >> (32 - sh));
         }
       }
-      if (in) edge(u, bs, j, re, v, pos, tail, hub, nbv);
+      if (hub) edge(u, bs, j, re, v, pos, tail, nbv, cost);
     }
   };
-  if (Mode == 2 && u1 - u0 < 32u * nwarps) {
+  if (Mode == 1 && u1 - u0 < 32u * nwarps) {
     // The in-list fill runs once per row wave; a wave of fewer rows than the
     // grid has lanes keeps every warp busy with one warp per row. Larger waves
     // (the first ones: millions of short rows) take the row-block loop below.
@@ -2129,9 +2132,10 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           }
           const uint32_t tail = nbu - pos;
           uint32_t nbv = 0;
-          const bool hub = Mode != 2 && hub_candidate<Mode>(vinfo, save, v, tail, nbv);
-          if (Mode == 1 && hub) atomicOr(&eflag[j >> 5], 1u << (j & 31));
-          edge(u, bs, j, re, v, pos, tail, hub, nbv);
+          unsigned long long cost = 0;
+          if (!decide(v, tail, nbv, cost)) continue;
+          if (Mode == 1) atomicOr(&eflag[j >> 5], 1u << (j & 31));
+          edge(u, bs, j, re, v, pos, tail, nbv, cost);
         }
       }
       // Longer rows: the warp, one row at a time.
@@ -2146,10 +2150,20 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   }
 }
 
-// Pieces per hub, 2n + 2 counts: cnt[v] CTA pieces of ceil(in-edges /
-// kHubPiece) for hubs wider than a warp's slice, cnt[n + 1 + v] warp pieces
-// of ceil(in-edges / kHubWarpPiece) for the rest; cnt[n] = cnt[2n + 1] = 0.
-// One exclusive scan places every CTA piece before every warp piece.
+// After mode 0: a hub whose candidates save at least its staging cost keeps
+// its candidate count (the length of its in-list) and is marked in save[v]
+// (1 << 32: the low word then counts its column tails in mode 1); any other
+// vertex gets no in-list.
+__global__ void k_hub_accept(const uint64_t* __restrict__ vinfo, uint32_t n, unsigned long long* __restrict__ save,
+                             uint32_t* __restrict__ in_cnt) {
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const uint64_t vi = vinfo[v];
+  const bool acc = in_cnt[v] > 0 && save[v] >= hub_cost((uint32_t)(vi >> 32), (uint32_t)vi);
+  if (!acc) in_cnt[v] = 0;
+  save[v] = acc ? (1ull << 32) : 0ull;
+}
+
 __global__ void k_hub_piece_count(const uint32_t* __restrict__ in_off, const uint64_t* __restrict__ vinfo,
                                   uint32_t n, uint32_t* __restrict__ cnt) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2320,26 +2334,26 @@ static void build_hubs(const GraphView& g, Schedule& s, cudaStream_t st) {
   TB_CUDA(cudaMemsetAsync(s.save, 0, n * sizeof(unsigned long long), st));
   TB_CUDA(cudaMemsetAsync(s.eflag, 0, (s.eflag_words) * sizeof(uint32_t), st));
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
+  // Candidates counted and savings summed in one pass; each hub accepted or
+  // not as a whole; its in-list sized by its candidates, then filled.
   k_hub_edges<0><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow, nullptr);
+                                           nullptr, nullptr);
   TB_LAUNCH_CHECK();
-  k_hub_edges<1><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
-                                           s.inrow, nullptr);
+  k_hub_accept<<<vblocks, 256, 0, st>>>(s.vinfo, (uint32_t)n, s.save, s.in_cnt);
   TB_LAUNCH_CHECK();
   device_scan<uint32_t, OpSum>(s.in_cnt, s.in_off, n + 1, true, OpSum{}, 0u, s.row_scan_tmp, st);
   TB_CUDA(cudaMemsetAsync(s.in_cnt, 0, (n + 1) * sizeof(uint32_t), st));
   k_wave_bounds<<<1, kHubWaves + 1, 0, st>>>(g, s.wave_lo, s.wave_bk, s.wave_cp);
-  if (kHubColRatio) TB_CUDA(cudaMemsetAsync(s.save, 0, n * sizeof(unsigned long long), st));  // column-tail counts
   TB_LAUNCH_CHECK();
   if (s.inl_cap <= kHubOneWaveEntries) {
     // A graph whose bit rows fit the L2 many times over gains nothing from
     // the wave order: one launch fills every in-list.
-    k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+    k_hub_edges<1><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
                                              s.hub_rows ? s.inrow : nullptr, nullptr);
     TB_LAUNCH_CHECK();
   } else {
     for (uint32_t w = 0; w < kHubWaves; ++w) {  // in-lists filled wave by wave: ordered by wave
-      k_hub_edges<2><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
+      k_hub_edges<1><<<eblocks, 256, 0, st>>>(g, s.variant_of, s.vinfo, s.save, s.eflag, s.in_cnt, s.in_off, s.inl,
                                                s.hub_rows ? s.inrow : nullptr, s.wave_lo + w);
       TB_LAUNCH_CHECK();
     }
