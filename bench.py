@@ -209,24 +209,36 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     c.capture_count()
     s = torch.cuda.Stream(device=local)
     c.set_stream(s.cuda_stream)
-    ms = []
-    for _ in range(steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        c.launch_count()
-        b.record(s)
-        b.synchronize()
-        ms.append(a.elapsed_time(b))
-    replay = c.batch_counts(num_graphs)
-    assert np.array_equal(replay, counts), "graph replay changed the per-graph counts"
+
+    def replay_ms():
+        out = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            c.launch_count()
+            b.record(s)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        assert np.array_equal(c.batch_counts(num_graphs), counts), "graph replay changed the per-graph counts"
+        return statistics.median(out)
+
+    ms = replay_ms()
+    # The other launch model at the same tuning: the row pieces and hub pass
+    # in one persistent kernel over the device work queue, or one per variant.
+    tuned_model = tb.LAUNCH_MODELS[tune.launch_model]
+    other = "queue" if tuned_model == "kernels" else "kernels"
+    c.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz, launch_model=other)
+    c.capture_count()
+    by_model = {tuned_model: ms, other: replay_ms()}
     c.close()
     # One graph at a time (a strided sample), same library, same stream model.
     d = torch.from_numpy(e.view(np.int64)).to(f"cuda:{local}")
     c1 = tb.Counter(device=local, dispatch=dispatch)
     if dispatch == "learned":
         c1.load_model(model_path)
-    c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz,  # the batch's tuned settings
-                  launch_model=tb.LAUNCH_MODELS[tune.launch_model])
+    # The batch's tuned settings, each graph's launch model chosen by its size
+    # (small graphs: the queue kernel).
+    c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz, launch_model="auto")
     idx = np.linspace(0, num_graphs - 1, per_graph_sample).astype(int)
     k_ms, e2e_one = 0.0, 0.0
     for g in idx:
@@ -239,7 +251,7 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
         assert rg.triangles == int(counts[g]), f"graph {g}: batch {counts[g]} vs single {rg.triangles}"
     c1.close()
     scale = num_graphs / per_graph_sample
-    batched_ms = statistics.median(ms)
+    batched_ms = ms
     return {
         "graphs": num_graphs, "entries": int(e.size), "edges": int(r.edges), "triangles": int(counts.sum()),
         "batched_count_ms": batched_ms, "graphs_per_s_batched": num_graphs / (batched_ms / 1e3),
@@ -247,6 +259,7 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
         "e2e_graphs_per_s_batched": num_graphs / e2e_s,
         "e2e_graphs_per_s_per_graph": num_graphs / (e2e_one * scale),
         "per_graph_sample": per_graph_sample, "tuning": tune.as_dict(), "cuda_graph": True,
+        "batched_count_ms_by_launch_model": by_model,
         "row_blocks_by_variant": dict(zip(tb.VARIANTS, r.row_blocks_by_variant)),
     }
 
