@@ -77,6 +77,12 @@ void run_call(tribit_context* c, tb::PrepInput in, const uint64_t* host_entries,
     pin.upload.copy_stream = c->copy_st;
     pin.upload.events = c->upload_ev;
     pin.upload.uploaded = c->ev[1];
+    // Pageable input of at least one 32 MiB staging piece: copied into the
+    // context's pinned buffers by host threads rather than by the driver.
+    if (in.E * sizeof(uint64_t) >= (32u << 20) && !tb::host_is_pinned(host_entries)) {
+      pin.upload.stage = &tb::stage_pageable;
+      pin.upload.stage_ctx = c;
+    }
   } else {
     TB_CUDA(cudaEventRecord(c->ev[1], st));
   }

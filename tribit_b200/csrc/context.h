@@ -45,6 +45,7 @@ struct tribit_context {
   tb::Arena load_arena;
   void* pinned[2] = {nullptr, nullptr};
   cudaEvent_t pinned_ev[2] = {};       // the last device copy that used pinned[b], on any stream
+  int pinned_turn = 0;                 // the pinned buffer the next staged piece takes
   const uint64_t* loaded_entries = nullptr;
   uint64_t loaded_E = 0, loaded_n = 0;
   bool loaded = false;
@@ -119,6 +120,12 @@ bool count_streamed_if_needed(tribit_context* c, const uint64_t* host, uint64_t 
 // Copies bytes of host memory to device memory through the context's two
 // pinned buffers (host threads fill one while the other's copy runs).
 void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst);
+// Whether host memory is pinned (page-locked or registered).
+bool host_is_pinned(const void* p);
+// HostUpload::stage for pageable host memory (ctx: the context): the bytes go
+// through the context's pinned buffers in turn, copied in by host threads
+// while the previous piece's copy runs, on stream st.
+void stage_pageable(void* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // The host writes or reads pinned buffer b only once the last device copy
 // that used it has finished; every such copy is followed by pinned_used.

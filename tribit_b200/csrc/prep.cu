@@ -702,7 +702,13 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
     uint64_t* dst = const_cast<uint64_t*>(in.entries);
     const bool upload = up.host && E > 0;
     const bool overlap = upload && by_degree && n > 0;
-    if (upload && !overlap) TB_CUDA(cudaMemcpyAsync(dst, up.host, E * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    auto copy = [&](uint64_t* to, const uint64_t* from, uint64_t words, cudaStream_t s) {
+      if (up.stage)
+        up.stage(up.stage_ctx, to, from, words * sizeof(uint64_t), s);
+      else
+        TB_CUDA(cudaMemcpyAsync(to, from, words * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    };
+    if (upload && !overlap) copy(dst, up.host, E, st);
     if (upload && !overlap && up.uploaded) TB_CUDA(cudaEventRecord(up.uploaded, st));
     if (by_degree && n > 0) {
       TB_CUDA(cudaMemsetAsync(deg, 0, n * sizeof(uint32_t), st));
@@ -715,8 +721,7 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
         for (int k = 0; k < kUploadChunks; ++k) {
           const uint64_t i0 = k * piece, i1 = std::min<uint64_t>(E, i0 + piece);
           if (i0 >= i1) break;
-          TB_CUDA(cudaMemcpyAsync(dst + i0, up.host + i0, (i1 - i0) * sizeof(uint64_t), cudaMemcpyHostToDevice,
-                                  up.copy_stream));
+          copy(dst + i0, up.host + i0, i1 - i0, up.copy_stream);
           TB_CUDA(cudaEventRecord(up.events[k + 1], up.copy_stream));
           TB_CUDA(cudaStreamWaitEvent(st, up.events[k + 1], 0));
           if (i1 == E && up.uploaded) TB_CUDA(cudaEventRecord(up.uploaded, st));

@@ -56,6 +56,11 @@ struct HostUpload {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t* events = nullptr;
   cudaEvent_t uploaded = nullptr;
+  // Optional: copies bytes from host to device on a stream in its own way
+  // (pageable host memory staged through pinned buffers by host threads);
+  // null: one cudaMemcpyAsync.
+  void (*stage)(void* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) = nullptr;
+  void* stage_ctx = nullptr;
 };
 
 struct PrepInput {

@@ -264,12 +264,6 @@ float ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-bool host_is_pinned(const void* p) {
-  cudaPointerAttributes pa{};
-  const bool pinned = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-  (void)cudaGetLastError();
-  return pinned;
-}
 
 // Host entries streamed through two device piece buffers: pass(fn) calls
 // fn(piece, count) per piece on the context's stream. Pinned host entries are
@@ -323,6 +317,28 @@ struct PieceStream {
 };
 
 }  // namespace
+
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes pa{};
+  const bool pinned = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();
+  return pinned;
+}
+
+void stage_pageable(void* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  tribit_context* c = static_cast<tribit_context*>(ctx);
+  ensure_pinned(c);
+  const size_t piece = kPieceWords * sizeof(uint64_t);
+  for (size_t at = 0; at < bytes; at += piece) {
+    const size_t len = std::min(piece, bytes - at);
+    const int b = c->pinned_turn;
+    c->pinned_turn ^= 1;
+    pinned_wait(c, b);
+    host_copy(c->pinned[b], (const char*)src + at, len);
+    TB_CUDA(cudaMemcpyAsync((char*)dst + at, c->pinned[b], len, cudaMemcpyHostToDevice, st));
+    pinned_used(c, b, st);
+  }
+}
 
 void upload_via_pinned(tribit_context* c, const void* src, size_t bytes, void* dst) {
   ensure_pinned(c);
