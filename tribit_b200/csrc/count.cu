@@ -267,6 +267,11 @@ __device__ __forceinline__ uint64_t sweep(const GraphView& g, uint32_t cs, uint3
 #define TB_BITS_DEPTH 4
 #endif
 constexpr int kBitsDepth = TB_BITS_DEPTH;
+// Column id w as a one-bit entry of its block; `keep` false: the block alone
+// (matches nothing).
+__device__ __forceinline__ uint64_t col_entry(uint32_t w, bool keep) {
+  return ((uint64_t)(w >> 5) << 32) | (keep ? 1u << (w & 31) : 0u);
+}
 
 template <class Probe>
 __device__ __forceinline__ uint64_t sweep_bits(const GraphView& g, uint32_t cs, uint32_t ce, uint32_t chunk0,
@@ -1389,12 +1394,6 @@ __device__ __forceinline__ uint64_t sweep_tail_pairs(const GraphView& g, const u
   }
   __syncwarp();
   return acc;
-}
-
-// Column id w as a one-bit entry of its block; `keep` false: the block alone
-// (matches nothing).
-__device__ __forceinline__ uint64_t col_entry(uint32_t w, bool keep) {
-  return ((uint64_t)(w >> 5) << 32) | (keep ? 1u << (w & 31) : 0u);
 }
 
 // Column tails (in-list entries (first CSR position << 32) | neighbours): u's

@@ -6,9 +6,11 @@ three times from device memory (median preprocessing time); then
 write that flushes the L2, timed with CUDA events on that stream; the first
 three are warm-up. Prints one JSON line: the median and minimum counting time,
 the preprocessing time, the count and the dispatcher's row blocks per variant.
+`--gen batch` is the benchmark's 4,096-graph batch, prepared from host memory
+by tribit_count_batch (tiles off, 7 CTAs an SM, 128-neighbour pieces).
 
   python -m tribit_b200.measure --scale 24 --seed 24 [--dispatch learned]
-      [--model PATH] [--gen rmat|planted|er|er_small|c1] [--launch-model kernels|queue|auto]
+      [--model PATH] [--gen rmat|planted|er|er_small|c1|batch] [--launch-model kernels|queue|auto]
       [--steps 10] [--tag NAME]
 
 This is the launch-timing loop the profiles under `profiles/` cite; `bench.py`
@@ -51,23 +53,32 @@ def main():
     ap.add_argument("--seed", type=int, default=24)
     ap.add_argument("--dispatch", default="learned", choices=sorted(tb.DISPATCH))
     ap.add_argument("--model", default=os.path.join(HERE, "models", "dispatch_mlp.bin"))
-    ap.add_argument("--gen", default="rmat", choices=["rmat", "planted", "er", "er_small", "c1"])
+    ap.add_argument("--gen", default="rmat", choices=["rmat", "planted", "er", "er_small", "c1", "batch"])
     ap.add_argument("--launch-model", default="auto", choices=list(tb.LAUNCH_MODELS))
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--tag", default="")
     a = ap.parse_args()
 
-    n, e = workload(a.gen, a.scale, a.seed)
-    d = torch.from_numpy(e.view(np.int64)).cuda()
+    batch = a.gen == "batch"
+    if batch:  # the 4,096-graph batch of the benchmark, tiles off, 7 CTAs an SM, 128-neighbour pieces
+        e, off, nn = tb.gen_batch(4096, seed=4096)
+    else:
+        n, e = workload(a.gen, a.scale, a.seed)
+        d = torch.from_numpy(e.view(np.int64)).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     s = torch.cuda.Stream()
     with tb.Counter(dispatch=a.dispatch) as c:
         if a.dispatch == "learned":
             c.load_model(a.model)
         c.set_stream(s.cuda_stream)
-        c.set_tuning(0, 64, 64.0, launch_model=a.launch_model)
-        c.prepare_device(d.data_ptr(), d.numel(), n)
-        prep = [c.prepare_device(d.data_ptr(), d.numel(), n).preprocess_ms for _ in range(3)]
+        if batch:
+            c.set_tuning(7, 128, 1e30, launch_model=a.launch_model)
+            c.count_batch(e, off, nn)
+            prep = [c.count_batch(e, off, nn)[1].preprocess_ms for _ in range(3)]
+        else:
+            c.set_tuning(0, 64, 64.0, launch_model=a.launch_model)
+            c.prepare_device(d.data_ptr(), d.numel(), n)
+            prep = [c.prepare_device(d.data_ptr(), d.numel(), n).preprocess_ms for _ in range(3)]
         ms = []
         with torch.cuda.stream(s):
             for k in range(a.steps + 3):
