@@ -2023,11 +2023,12 @@ __device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo
 // is below the staging cost: the decision save[v] >= cost (k_hub_accept) is
 // then the one the full sum gives, without one atomic per in-edge on the
 // most popular hubs.
-// Mode 1: every candidate edge of an accepted hub (save[v] >> 32 set) is
-// flagged and appended to the hub's in-list: a bit-row tail (first block,
-// blocks) at the front (in_cnt[v] counts them), a column tail (first CSR
-// position after v, neighbours) at the back (the low word of save[v] counts
-// them). rows (may be null): the pass covers rows [rows[0], rows[1]).
+// Mode 1: every candidate edge of an accepted hub (a vertex whose vinfo
+// k_hub_accept kept) is flagged and appended to the hub's in-list: a bit-row
+// tail (first block, blocks) at the front (in_cnt[v] counts them), a column
+// tail (first CSR position after v, neighbours) at the back (the low word of
+// save[v] counts them). rows (may be null): the pass covers rows
+// [rows[0], rows[1]).
 constexpr uint32_t kHubLaneRow = 64;
 
 template <int Mode>
@@ -2041,11 +2042,10 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
   // Whether the edge to v (tail blocks) takes part: mode 0, a candidate;
-  // mode 1, a candidate of an accepted hub.
+  // mode 1, a candidate of an accepted hub (k_hub_accept clears the vinfo of
+  // every other vertex, so one read decides).
   auto decide = [&](uint32_t v, uint32_t tail, uint32_t& nbv, unsigned long long& cost) -> bool {
-    const bool cand = hub_candidate(vinfo, v, tail, nbv, cost);
-    if (Mode == 0) return cand;
-    return cand && (save[v] >> 32) != 0;
+    return hub_candidate(vinfo, v, tail, nbv, cost);
   };
   // Applies mode Mode to the taking-part edge at j (v = col[j]; u's row ends
   // at CSR position re) of row u.
@@ -2122,7 +2122,9 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
       }
       const bool own = mine && re - rs <= kHubLaneRow;
       if (own) {
-        uint32_t pos = 0xFFFFFFFFu, prev = 0xFFFFFFFFu;
+        // Mode 1 gathers the row's flag bits word by word: one atomicOr per
+        // 32 CSR positions (a word may hold the ends of other lanes' rows).
+        uint32_t pos = 0xFFFFFFFFu, prev = 0xFFFFFFFFu, fw = 0xFFFFFFFFu, fb = 0;
         for (uint32_t j = rs; j < re; ++j) {
           const uint32_t v = g.col[j];
           if ((v >> 5) != prev) {
@@ -2133,9 +2135,17 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
           uint32_t nbv = 0;
           unsigned long long cost = 0;
           if (!decide(v, tail, nbv, cost)) continue;
-          if (Mode == 1) atomicOr(&eflag[j >> 5], 1u << (j & 31));
+          if (Mode == 1) {
+            if ((j >> 5) != fw) {
+              if (fb) atomicOr(&eflag[fw], fb);
+              fw = j >> 5;
+              fb = 0;
+            }
+            fb |= 1u << (j & 31);
+          }
           edge(u, bs, j, re, v, pos, tail, nbv, cost);
         }
+        if (Mode == 1 && fb) atomicOr(&eflag[fw], fb);
       }
       // Longer rows: the warp, one row at a time.
       uint32_t longm = __ballot_sync(kFull, mine && !own);
@@ -2152,14 +2162,18 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
 // After mode 0: a hub whose candidates save at least its staging cost keeps
 // its candidate count (the length of its in-list) and is marked in save[v]
 // (1 << 32: the low word then counts its column tails in mode 1); any other
-// vertex gets no in-list.
-__global__ void k_hub_accept(const uint64_t* __restrict__ vinfo, uint32_t n, unsigned long long* __restrict__ save,
+// vertex gets no in-list, and its vinfo is cleared so that mode 1 takes none
+// of its edges.
+__global__ void k_hub_accept(uint64_t* __restrict__ vinfo, uint32_t n, unsigned long long* __restrict__ save,
                              uint32_t* __restrict__ in_cnt) {
   const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= n) return;
   const uint64_t vi = vinfo[v];
   const bool acc = in_cnt[v] > 0 && save[v] >= hub_cost((uint32_t)(vi >> 32), (uint32_t)vi);
-  if (!acc) in_cnt[v] = 0;
+  if (!acc) {
+    in_cnt[v] = 0;
+    vinfo[v] = 0;  // no candidate in mode 1, no pieces
+  }
   save[v] = acc ? (1ull << 32) : 0ull;
 }
 
