@@ -2030,6 +2030,14 @@ __device__ __forceinline__ bool hub_candidate(const uint64_t* __restrict__ vinfo
 // save[v] counts them). rows (may be null): the pass covers rows
 // [rows[0], rows[1]).
 constexpr uint32_t kHubLaneRow = 64;
+#ifndef TB_HUB_TOP
+#define TB_HUB_TOP 1024
+#endif
+// Mode 0 counts the in-edges of the kHubTop highest-ranked vertices in shared
+// memory (under degree order they take a fifth to a third of all in-edges, so
+// their global counters would see the most contended atomics), one flush per
+// CTA.
+constexpr uint32_t kHubTop = TB_HUB_TOP;
 
 template <int Mode>
 __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of, const uint64_t* __restrict__ vinfo,
@@ -2041,6 +2049,18 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t u0 = rows ? rows[0] : 0u, u1 = rows ? rows[1] : g.n;  // rows [u0, u1)
+  // Mode 0: candidate counts and savings of the vertices ranked top_lo and
+  // above, per CTA. A CTA adds to a saving only while it is below the cost,
+  // as the global sums do, so a CTA's partial sum either is exact or already
+  // reaches the cost by itself: the decision save[v] >= cost is unchanged.
+  // Bounded: at most blockDim.x adds of at most nbv each past the cost.
+  constexpr uint32_t kTop = Mode == 0 ? kHubTop : 0u;
+  __shared__ uint32_t s_top[kTop ? 2 * kTop : 1];
+  const uint32_t top_lo = g.n > kTop ? g.n - kTop : 0u;
+  if (kTop) {
+    for (uint32_t t = threadIdx.x; t < 2 * kTop; t += blockDim.x) s_top[t] = 0;
+    __syncthreads();
+  }
   // Whether the edge to v (tail blocks) takes part: mode 0, a candidate;
   // mode 1, a candidate of an accepted hub (k_hub_accept clears the vinfo of
   // every other vertex, so one read decides).
@@ -2052,6 +2072,12 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   auto edge = [&](uint32_t u, uint32_t bs, uint32_t j, uint32_t re, uint32_t v, uint32_t pos, uint32_t tail,
                   uint32_t nbv, unsigned long long cost) {
     if (Mode == 0) {
+      if (kTop && v >= top_lo) {
+        uint32_t* c = s_top + 2 * (v - top_lo);
+        atomicAdd(c, 1u);
+        if (*(volatile uint32_t*)(c + 1) < cost) atomicAdd(c + 1, nbv - tail);
+        return;
+      }
       atomicAdd(&in_cnt[v], 1u);
       if (*(volatile const unsigned long long*)&save[v] < cost) atomicAdd(&save[v], (unsigned long long)(nbv - tail));
     } else {
@@ -2155,6 +2181,14 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
         warp_row(rb * 32 + r, __shfl_sync(kFull, rs, r), __shfl_sync(kFull, re, r), __shfl_sync(kFull, bs, r),
                  __shfl_sync(kFull, nbu, r));
       }
+    }
+  }
+  if (kTop) {
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < kTop && top_lo + t < g.n; t += blockDim.x) {
+      const uint32_t c = s_top[2 * t], sv = s_top[2 * t + 1];
+      if (c) atomicAdd(&in_cnt[top_lo + t], c);
+      if (sv) atomicAdd(&save[top_lo + t], (unsigned long long)sv);
     }
   }
 }
