@@ -8,7 +8,8 @@ data of that shape generated on the host. A step is one launch of the counting
 kernels over the prepared (oriented, bit-packed) graph already resident in
 HBM; preprocessing is timed separately, as the reference reports it. `e2e` is
 the same metric through the public C-ABI call tribit_count_edges on pinned
-host entries: H2D copy, preprocessing, counting and the D2H result inside.
+host entries: H2D copy, preprocessing, counting and the D2H result inside,
+the mean wall time of --e2e-steps calls (5; each call's time in step_ms).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload rmat24|rmat22|rmat20|chung_lu|planted]
@@ -355,7 +356,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
     ap.add_argument("--dispatch", default="auto")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4,096-graph batch measurement")
     ap.add_argument("--stream-budgets", default="0.5,0.3",
@@ -479,12 +480,12 @@ def main():
             secs.append(time.perf_counter() - t1)
         c.close()
         assert last.triangles == res.triangles
-        return reduce_replicas(dist, m, statistics.mean(secs), device)[1], last
+        return reduce_replicas(dist, m, statistics.mean(secs), device)[1], last, secs
 
-    e2e_t, e2e_res = e2e_run(dispatch)
+    e2e_t, e2e_res, e2e_secs = e2e_run(dispatch)
     e2e_by_mode = {dispatch: job_edges / e2e_t}
     if dispatch == "learned":
-        t_plain, _ = e2e_run("plain")
+        t_plain, _, _ = e2e_run("plain")
         e2e_by_mode["plain"] = job_edges / t_plain
 
     def streamed_run(item):
@@ -566,6 +567,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": job_edges / e2e_t, "unit": "edges/s", "h2d_bytes_per_step": int(entries.size) * 8,
                     "d2h_bytes_per_step": 108, "ms_per_step": e2e_t * 1e3,
+                    # wall time of each call on this rank (ms_per_step: their mean, slowest rank)
+                    "step_ms": [round(t * 1e3, 2) for t in e2e_secs],
                     # device-timed parts of the last call (the degree pass overlaps the upload)
                     "parts_ms": {"h2d": e2e_res.h2d_ms, "preprocess": e2e_res.preprocess_ms,
                                  "count": e2e_res.kernel_ms},
