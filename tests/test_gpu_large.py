@@ -43,6 +43,24 @@ def test_rmat24_vs_oracle():
             assert (r.triangles, r.edges) == (want, m), mode
 
 
+def test_degree_slot_rows_with_duplicates_and_loops():
+    """Inputs of 2^27 entries or more build their rows in degree-sized slots:
+    33 copies of RMAT-18 (every other one reversed) plus self-loops, so rows
+    hold tens of thousands of entries before deduplication and are sorted in
+    global scratch. The simple graph, and so the count, is RMAT-18's."""
+    n = 1 << 18
+    base = tb.gen_rmat(18, 16, seed=18)
+    rev = (base << np.uint64(32)) | (base >> np.uint64(32))
+    loops = (np.arange(1000, dtype=np.uint64) << np.uint64(32)) | np.arange(1000, dtype=np.uint64)
+    e = np.concatenate([base if k % 2 == 0 else rev for k in range(33)] + [loops])
+    assert e.size >= 1 << 27
+    want = oracle.count(base, n)
+    for mode in ("plain", "merge"):
+        with tb.Counter(dispatch=mode) as c:
+            r = c.count_edges(e, n)
+            assert (r.triangles, r.edges) == want, mode
+
+
 def test_rmat22_modes_agree():
     e = tb.gen_rmat(22, 16, seed=22)
     got = set()

@@ -2057,7 +2057,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
   constexpr uint32_t kTop = Mode == 0 ? kHubTop : 0u;
   __shared__ uint32_t s_top[kTop ? 2 * kTop : 1];
   const uint32_t top_lo = g.n > kTop ? g.n - kTop : 0u;
-  if (kTop) {
+  if constexpr (kTop != 0) {
     for (uint32_t t = threadIdx.x; t < 2 * kTop; t += blockDim.x) s_top[t] = 0;
     __syncthreads();
   }
@@ -2183,7 +2183,7 @@ __global__ void k_hub_edges(GraphView g, const uint8_t* __restrict__ variant_of,
       }
     }
   }
-  if (kTop) {
+  if constexpr (kTop != 0) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < kTop && top_lo + t < g.n; t += blockDim.x) {
       const uint32_t c = s_top[2 * t], sv = s_top[2 * t + 1];

@@ -157,6 +157,47 @@ __global__ void k_row_fill(const uint64_t* __restrict__ keys, uint64_t E, uint32
   }
 }
 
+// Slot path (inputs that take the presort, under degree order): row r is
+// given a slot of deg(v) entries, v the vertex of rank r (every entry oriented
+// from v is one of the deg(v) entries that touch v), so no pass counts the
+// rows: cap[r] = deg(v), cap[n] = 0, scanned to the slot starts.
+__global__ void k_slot_sizes(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ rank, uint64_t n,
+                             uint32_t* __restrict__ cap) {
+  const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) cap[rank[v]] = deg[v];
+  if (v == n) cap[n] = 0;
+}
+
+// Slot path: keys[i] = (lo << 32) | hi of entry i (kDropped for a dropped
+// entry), over the presort's radix tiles, each tile also counting its keys'
+// presort digits (key >> shift) & 255 into hist (digit-major, as k_radix_hist
+// leaves them): the keys and the presort's histogram in one pass.
+__global__ void __launch_bounds__(kSortThreads) k_row_keys_hist(PrepInput in, const uint32_t* __restrict__ rank,
+                                                                 uint64_t* __restrict__ keys, int shift,
+                                                                 uint32_t tiles, uint32_t* __restrict__ hist,
+                                                                 unsigned int* err) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int j = 0; j < kSortKeysPerThread; ++j) {
+    const uint64_t i = base + (uint64_t)j * kSortThreads + threadIdx.x;
+    uint32_t d = 256u;
+    if (i < in.E) {
+      uint32_t lo, hi;
+      uint64_t key = kDropped;
+      if (orient_entry(in, rank, i, lo, hi, err)) key = ((uint64_t)lo << 32) | hi;
+      keys[i] = key;
+      d = (uint32_t)((key >> shift) & 255);
+    }
+    const uint32_t peers = __match_any_sync(kFull, d);
+    if (d < 256 && (threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  hist[(uint64_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
 #ifndef TB_PRESORT_MIN
 #define TB_PRESORT_MIN (1ull << 27)
 #endif
@@ -278,12 +319,13 @@ __device__ __forceinline__ void sort_short_rows(uint32_t pending, uint32_t s_l, 
 
 // One warp per 32-row block: rows of up to 8 and 16 entries are sorted four
 // and two at a time in lane groups, rows of up to kWarpSortMax one at a time
-// in registers; longer rows go to big[] for k_sort_big_rows. rows[u] =
-// (distinct << 32) | blocks, rows[n] = 0.
+// in registers; longer rows go to big[] for k_sort_big_rows. Row u holds
+// nbr[start[u], end[u]). rows[u] = (distinct << 32) | blocks, rows[n] = 0.
 // (Four CTAs of 256 per SM: 64 registers, no spills.)
 __global__ void __launch_bounds__(256, 4)
-    k_sort_rows(const uint32_t* __restrict__ off, uint32_t n, uint32_t* __restrict__ nbr, uint64_t* __restrict__ rows,
-                uint32_t* __restrict__ big, uint32_t* __restrict__ nbig) {
+    k_sort_rows(const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, uint32_t n,
+                uint32_t* __restrict__ nbr, uint64_t* __restrict__ rows, uint32_t* __restrict__ big,
+                uint32_t* __restrict__ nbig) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -291,7 +333,7 @@ __global__ void __launch_bounds__(256, 4)
   for (uint32_t ubase = warp * 32; ubase < n; ubase += nwarps * 32) {
     const uint32_t u = ubase + lane;
     const bool here = u < n;
-    const uint32_t s_l = here ? off[u] : 0u, L_l = here ? off[u + 1] - s_l : 0u;
+    const uint32_t s_l = here ? start[u] : 0u, L_l = here ? end[u] - s_l : 0u;
     if (here && L_l == 0) rows[u] = 0;
     sort_short_rows<8>(__ballot_sync(kFull, L_l >= 1 && L_l <= 8), s_l, L_l, ubase, nbr, rows);
     sort_short_rows<16>(__ballot_sync(kFull, L_l > 8 && L_l <= 16), s_l, L_l, ubase, nbr, rows);
@@ -324,9 +366,11 @@ __global__ void __launch_bounds__(256, 4)
 
 // Rows longer than kWarpSortMax, one CTA per row: a bitonic sort of the row
 // padded to a power of two P, in shared memory (P <= kCtaSortSmem) or in the
-// row's slice [2 s, 2 s + P) of scratch (P <= 2 L), then the distinct values
-// written back to the front of the row.
-__global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_t* __restrict__ off,
+// row's slice [2 s, 2 s + P) of scratch (P <= 2 L; scratch holds twice the
+// entries nbr's row slots hold), then the distinct values written back to the
+// front of the row.
+__global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_t* __restrict__ start,
+                                                                   const uint32_t* __restrict__ end,
                                                                    uint32_t* __restrict__ nbr,
                                                                    uint32_t* __restrict__ scratch,
                                                                    uint64_t* __restrict__ rows,
@@ -338,7 +382,7 @@ __global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_
   const uint32_t count = *nbig;
   for (uint32_t bi = blockIdx.x; bi < count; bi += gridDim.x) {
     const uint32_t u = big[bi];
-    const uint32_t s = off[u], L = off[u + 1] - s;
+    const uint32_t s = start[u], L = end[u] - s;
     uint32_t P = 1;
     while (P < L) P <<= 1;
     uint32_t* a = P <= kCtaSortSmem ? sm : scratch + 2ull * s;
@@ -389,7 +433,7 @@ __global__ void __launch_bounds__(kCtaSortThreads) k_sort_big_rows(const uint32_
   }
 }
 
-// The row's distinct sorted values (front of its nbr slice) to col, and its
+// The row's distinct sorted values (front of its nbr slice, from off[u]) to col, and its
 // bit-row entries (block << 32 | mask) to bent, each written once. One warp
 // per 32 rows: a row of at most kLaneEmit values is written by its own lane;
 // a longer one by the whole warp, where the mask of a block is a segmented OR
@@ -521,19 +565,34 @@ __global__ void k_range_carry(uint64_t* __restrict__ rp, uint32_t count, const u
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) rp[k] += c;
 }
 
-void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t st, Prepared* out,
-              DeviceStats* stats, uint64_t* rp) {
+void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, const uint32_t* deg, cudaStream_t st,
+              Prepared* out, DeviceStats* stats, uint64_t* rp) {
   const uint64_t E = in.E, n = in.n;
-  uint32_t* cnt = ar.take<uint32_t>(n + 1);  // row lengths, then the fill cursors
-  uint32_t* off = ar.take<uint32_t>(n + 1);
+  const bool presort = E >= kPresortMinEntries && n > 256;
+  // Slot path: with full degrees, rows take degree-sized slots (2E entries
+  // in all, u32 offsets) and the keys' presort histogram is counted while they
+  // are written: no per-row atomics, no separate histogram pass (RMAT-24:
+  // row counts 2.9 ms and the histogram 1.0 ms, for 1 GB more of nbr).
+  // (Decided from the order, not from deg: the arena's measuring pass hands
+  // out null buffers and must plan the same layout.)
+  const bool slots =
+      presort && in.order == TRIBIT_ORDER_DEGREE && kDegreeSample == 1 && 2 * E < 0xFFFFFFFFull;
+  const uint64_t cap = slots ? 2 * E : E;  // nbr entries
+  uint32_t* cnt = ar.take<uint32_t>(n + 1);  // row lengths or slot sizes, then the fill cursors: the row ends
+  uint32_t* off = ar.take<uint32_t>(n + 1);  // row starts
   uint32_t* otmp = take_scan_temp<uint32_t>(ar, n + 1);
   uint64_t* rtmp = take_scan_temp<uint64_t>(ar, n + 1);
   uint32_t* big = ar.take<uint32_t>(n + 1);
   uint32_t* nbig = ar.take<uint32_t>(1);
-  uint32_t* nbr = ar.take<uint32_t>(E ? E : 1);
-  uint32_t* scratch = ar.take<uint32_t>(2 * E + 2);  // the oriented keys, then long rows' sort space
-  const bool presort = E >= kPresortMinEntries && n > 256;
-  uint64_t* keys_alt = presort ? ar.take<uint64_t>(E) : nullptr;
+  uint32_t* nbr = ar.take<uint32_t>(cap ? cap : 1);
+  // The oriented keys (on the slot path both presort buffers), then long
+  // rows' sort space (twice nbr).
+  uint32_t* scratch = ar.take<uint32_t>(2 * cap + 2);
+  uint64_t* keys_alt = nullptr;
+  if (slots)
+    keys_alt = reinterpret_cast<uint64_t*>(scratch + 2 * E + 2);
+  else if (presort)
+    keys_alt = ar.take<uint64_t>(E);
   RadixTemp ktmp;
   if (presort) ktmp = take_radix_temp(ar, E);
   uint32_t* col = ar.take<uint32_t>(E + 4);   // + 4: 16-byte quad loads may read three ids past the end
@@ -544,31 +603,41 @@ void run_rows(Arena& ar, const PrepInput& in, const uint32_t* rank, cudaStream_t
 
   const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(n, 8), 148ull * 32));
   uint64_t* keys = reinterpret_cast<uint64_t*>(scratch);
-  TB_CUDA(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), st));
+  const int top = 32 + bits_for(n) - 8;  // the presort digit: the top 8 bits of lo
   TB_CUDA(cudaMemsetAsync(nbig, 0, sizeof(uint32_t), st));
-  if (E > 0) {
-    k_row_count<<<grid_for(E, 8), kThreads, 0, st>>>(in, rank, cnt, keys, &stats->err);
+  if (slots) {
+    k_slot_sizes<<<grid_for(n + 1), kThreads, 0, st>>>(deg, rank, n, cnt);
     TB_LAUNCH_CHECK();
+    device_scan<uint32_t, OpSum>(cnt, off, n + 1, true, OpSum{}, 0u, otmp, st);
+    const uint64_t tiles = ceil_div<uint64_t>(E, kSortTile);
+    k_row_keys_hist<<<(unsigned)tiles, kSortThreads, 0, st>>>(in, rank, keys, top, (uint32_t)tiles, ktmp.hist,
+                                                               &stats->err);
+    TB_LAUNCH_CHECK();
+  } else {
+    TB_CUDA(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), st));
+    if (E > 0) {
+      k_row_count<<<grid_for(E, 8), kThreads, 0, st>>>(in, rank, cnt, keys, &stats->err);
+      TB_LAUNCH_CHECK();
+    }
+    device_scan<uint32_t, OpSum>(cnt, off, n + 1, true, OpSum{}, 0u, otmp, st);
   }
-  device_scan<uint32_t, OpSum>(cnt, off, n + 1, true, OpSum{}, 0u, otmp, st);
   if (E > 0) {
     // One radix pass on the top 8 bits of lo groups the keys into 256 ranges
     // of rows, so the fill's cursors and stores at any time stay in one
     // range's few MB of L2 instead of scattering over all rows.
     const uint64_t* fill_keys = keys;
-    if (presort) {
-      const int top = 32 + bits_for(n) - 8;
+    if (presort)
       fill_keys = radix_sort<uint64_t, NoVal, false>(keys, keys_alt, nullptr, nullptr, E, top + 8, ktmp, st, nullptr,
-                                                     top);
-    }
+                                                     top, slots);
     TB_CUDA(cudaMemcpyAsync(cnt, off, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     k_row_fill<<<grid_for(E, 8), kThreads, 0, st>>>(fill_keys, E, cnt, nbr);
     TB_LAUNCH_CHECK();
   }
-  k_sort_rows<<<wgrid, kThreads, 0, st>>>(off, (uint32_t)n, nbr, rp, big, nbig);
+  // Row u: nbr[off[u], cnt[u]) (with no entries every row is empty: 0, 0).
+  k_sort_rows<<<wgrid, kThreads, 0, st>>>(off, cnt, (uint32_t)n, nbr, rp, big, nbig);
   TB_LAUNCH_CHECK();
   if (E > kWarpSortMax) {
-    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(off, nbr, scratch, rp, big, nbig);
+    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(off, cnt, nbr, scratch, rp, big, nbig);
     TB_LAUNCH_CHECK();
   }
   device_scan<uint64_t, OpSum>(rp, rp, n + 1, true, OpSum{}, 0ull, rtmp, st);
@@ -614,10 +683,11 @@ void finish_row_range(const RowRangeBuffers& b, uint32_t s, uint32_t z, uint64_t
   k_range_check<<<grid_for(z), kThreads, 0, st>>>(b.off, b.cursor, z, err);
   TB_LAUNCH_CHECK();
   const unsigned wgrid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(z, 8), 148ull * 32));
-  k_sort_rows<<<wgrid, kThreads, 0, st>>>(b.off, z, b.nbr, rp + s, b.big, b.nbig);
+  k_sort_rows<<<wgrid, kThreads, 0, st>>>(b.off, b.off + 1, z, b.nbr, rp + s, b.big, b.nbig);
   TB_LAUNCH_CHECK();
   if (cnt > kWarpSortMax) {
-    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(b.off, b.nbr, b.scratch, rp + s, b.big, b.nbig);
+    k_sort_big_rows<<<148 * 2, kCtaSortThreads, 0, st>>>(b.off, b.off + 1, b.nbr, b.scratch, rp + s, b.big,
+                                                         b.nbig);
     TB_LAUNCH_CHECK();
   }
   device_scan<uint64_t, OpSum>(rp + s, rp + s, (uint64_t)z + 1, true, OpSum{}, 0ull, b.scan_tmp, st);
@@ -747,7 +817,7 @@ void prepare_graph(Arena& ar, const PrepInput& in, cudaStream_t st, Prepared* ou
     }
   }
   // Phase 2: orient, rows, sort + dedup per row, CSR + bit rows.
-  run_rows(ar, in, rank, st, out, stats, rp);
+  run_rows(ar, in, rank, deg, st, out, stats, rp);
 }
 
 }  // namespace tb

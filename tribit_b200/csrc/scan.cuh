@@ -280,10 +280,12 @@ inline RadixTemp take_radix_temp(Arena& ar, uint64_t n) {
 // Sorts keys[0, n) on bits [begin_bit, end_bit) (stable). keys_alt (and
 // vals_alt) are scratch of the same size. Returns the buffer that holds the
 // sorted keys (keys or keys_alt); *vals_sorted receives the matching values
-// buffer. Launches only.
+// buffer. first_hist_ready: tmp.hist already holds the first pass's per-tile
+// digit counts (digit-major, k_radix_hist's layout), counted by the kernel that
+// wrote the keys. Launches only.
 template <typename K, typename V, bool HasVals>
 K* radix_sort(K* keys, K* keys_alt, V* vals, V* vals_alt, uint64_t n, int end_bit, const RadixTemp& tmp,
-              cudaStream_t st, V** vals_sorted, int begin_bit = 0) {
+              cudaStream_t st, V** vals_sorted, int begin_bit = 0, bool first_hist_ready = false) {
   static_assert(sizeof(K) * kSortTile + (HasVals ? sizeof(V) * kSortTile : 0) + 4 * (kSortWarps * 256 + 512) <= 48 * 1024,
                 "radix scatter tile exceeds static shared memory");
   uint64_t tiles = ceil_div<uint64_t>(n, kSortTile);
@@ -292,8 +294,10 @@ K* radix_sort(K* keys, K* keys_alt, V* vals, V* vals_alt, uint64_t n, int end_bi
   V* vsrc = vals;
   V* vdst = vals_alt;
   for (int shift = begin_bit; n > 0 && shift < end_bit; shift += 8) {
-    k_radix_hist<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(src, n, shift, (uint32_t)tiles, tmp.hist);
-    TB_LAUNCH_CHECK();
+    if (!(first_hist_ready && shift == begin_bit)) {
+      k_radix_hist<K><<<(unsigned)tiles, kSortThreads, 0, st>>>(src, n, shift, (uint32_t)tiles, tmp.hist);
+      TB_LAUNCH_CHECK();
+    }
     device_scan<uint32_t, OpSum>(tmp.hist, tmp.hist, tiles * 256, true, OpSum{}, 0u, tmp.scan, st);
     k_radix_scatter<K, V, HasVals><<<(unsigned)tiles, kSortThreads, 0, st>>>(src, dst, vsrc, vdst, n, shift,
                                                                              (uint32_t)tiles, tmp.hist);
