@@ -9,7 +9,8 @@ kernels over the prepared (oriented, bit-packed) graph already resident in
 HBM; preprocessing is timed separately, as the reference reports it. `e2e` is
 the same metric through the public C-ABI call tribit_count_edges on pinned
 host entries: H2D copy, preprocessing, counting and the D2H result inside,
-the mean wall time of --e2e-steps calls (5; each call's time in step_ms).
+the mean wall time of --e2e-steps calls (5; each call's time in step_ms;
+Python's garbage collector run before each call and held off during it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload rmat24|rmat22|rmat20|chung_lu|planted]
@@ -30,6 +31,7 @@ oracle (a port), timed on a strided sample of 32-row blocks and extrapolated.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -111,6 +113,20 @@ def profiled_traffic(workload, dispatch):
             except ValueError:
                 return None
     return None
+
+
+def wall_call(fn):
+    """(fn(), its wall time in s), Python's garbage collector run before the
+    call and held off during it: the library call allocates no Python objects,
+    so a collection inside it would time the interpreter's heap, not the call."""
+    gc.collect()
+    gc.disable()
+    try:
+        t0 = time.perf_counter()
+        out = fn()
+        return out, time.perf_counter() - t0
+    finally:
+        gc.enable()
 
 
 class ClockSampler:
@@ -203,9 +219,7 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     if dispatch == "learned":
         c.load_model(model_path)
     counts, r = c.count_batch(host, off, nn)  # sizes the arena, prepares the batch
-    t0 = time.perf_counter()
-    counts, r = c.count_batch(host, off, nn)
-    e2e_s = time.perf_counter() - t0
+    (counts, r), e2e_s = wall_call(lambda: c.count_batch(host, off, nn))
     tune = c.autotune(reps=2)
     c.capture_count()
     s = torch.cuda.Stream(device=local)
@@ -245,9 +259,8 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     for g in idx:
         lo, hi = int(off[g]), int(off[g + 1])
         c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))  # sizes the arena
-        t1 = time.perf_counter()
-        rg = c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))
-        e2e_one += time.perf_counter() - t1
+        rg, dt = wall_call(lambda: c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g])))
+        e2e_one += dt
         k_ms += rg.kernel_ms
         assert rg.triangles == int(counts[g]), f"graph {g}: batch {counts[g]} vs single {rg.triangles}"
     c1.close()
@@ -475,9 +488,8 @@ def main():
         secs, last = [], None
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            last = c.count_edges(host, n)
-            secs.append(time.perf_counter() - t1)
+            last, dt = wall_call(lambda: c.count_edges(host, n))
+            secs.append(dt)
         c.close()
         assert last.triangles == res.triangles
         return reduce_replicas(dist, m, statistics.mean(secs), device)[1], last, secs
@@ -504,9 +516,8 @@ def main():
         secs, last = [], None
         for _ in range(2):
             torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            last = c.count_edges(src, n)
-            secs.append(time.perf_counter() - t1)
+            last, dt = wall_call(lambda: c.count_edges(src, n))
+            secs.append(dt)
         c.close()
         assert last.triangles == res.triangles
         t = reduce_replicas(dist, m, statistics.mean(secs), device)[1]
