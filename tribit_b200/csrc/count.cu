@@ -866,10 +866,11 @@ constexpr uint32_t kTcChunk = 256;                 // K bytes (columns) unpacked
 constexpr uint32_t kTcDrainPolls = 1u << 22;       // bounded wait for committed MMAs after a failed wait
 
 
+// 49 KiB: four CTAs an SM (128 of the 512 TMEM columns), so one CTA's
+// operand gathering runs while another's MMAs do.
 struct TcSmem {
   uint8_t a[kTileNbrPiece * kTcChunk];             // A: 128 rows x 256 K-bytes, core-matrix layout
   uint8_t b[32 * kTcChunk];                        // B: 32 rows x 256 K-bytes
-  uint32_t vbits[kTileNbrPiece][kTileMaxK];        // the neighbours' bits over the block's range
   uint32_t ubits[32][kTileMaxK];                   // the block's rows
   uint32_t vmask[kTileMaxK];                       // OR of the rows: V
   uint32_t vpre[kTileMaxK + 1];                    // popcount prefix of vmask
@@ -878,6 +879,8 @@ struct TcSmem {
   uint32_t tmem;
   uint32_t lo, K, amask, cnt_v, fail;
 };
+constexpr int kTcCtasPerSm = 4;
+static_assert(kTileMaxK == 64, "the vmask prefix is one warp scan of two words a lane");
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -987,13 +990,14 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
     const uint32_t K = sm.K, lo = sm.lo, amask = sm.amask;
     uint64_t racc = 0;
     if (K > (uint32_t)kTileMaxK) {
-      // Forced onto a block that fits no tile: its one piece sweeps the rows (warp 0).
+      // Forced onto a block that fits no tile: its one piece sweeps the rows
+      // (warp 0; the operand buffers are its table and run buffer).
       if (first == 0 && w == 0)
-        racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.vbits), sm.vpre, per_graph);
+        racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), reinterpret_cast<uint32_t*>(sm.b), per_graph);
     } else if (K > 0) {
       const uint32_t KW = (K + 7) & ~7u;  // words, whole 256-column chunks
-      for (uint32_t i = tid; i < 32 * kTileMaxK; i += kTcThreads) (&sm.ubits[0][0])[i] = 0u;
-      for (uint32_t i = tid; i < kTileNbrPiece * kTileMaxK; i += kTcThreads) (&sm.vbits[0][0])[i] = 0u;
+      for (uint32_t r = w; r < 32; r += kTcThreads / 32)
+        for (uint32_t q = lane; q < KW; q += 32) sm.ubits[r][q] = 0u;
       __syncthreads();
       // The rows' bits: warp w takes rows w, w + 4, ...
       for (uint32_t r = w; r < 32; r += 4) {
@@ -1011,20 +1015,23 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
         sm.vmask[tid] = m;
       }
       __syncthreads();
-      if (tid == 0) {
-        uint32_t run = 0;
-        for (uint32_t i = 0; i < (uint32_t)kTileMaxK; ++i) {
-          sm.vpre[i] = run;
-          run += __popc(sm.vmask[i]);
+      if (w == 0) {
+        const uint32_t c0 = __popc(sm.vmask[2 * lane]), c1 = __popc(sm.vmask[2 * lane + 1]);
+        const uint32_t incl = warp_inclusive_sum(c0 + c1);
+        sm.vpre[2 * lane] = incl - c0 - c1;
+        sm.vpre[2 * lane + 1] = incl - c1;
+        if (lane == 31) {
+          sm.vpre[kTileMaxK] = incl;
+          sm.cnt_v = min(kTileNbrPiece, incl > first ? incl - first : 0u);
         }
-        sm.vpre[kTileMaxK] = run;
-        sm.cnt_v = min(kTileNbrPiece, run > first ? run - first : 0u);
       }
       __syncthreads();
-      // Neighbour tid of the piece: the (first + tid)-th set bit of V; its
-      // bits over the range, gathered by this thread.
+      // Neighbour tid of the piece: the (first + tid)-th set bit of V. Its
+      // bit row starts at or after block lo (v >= 32 lo) and ascends, so a
+      // cursor walks it chunk by chunk: a chunk's 8 words hold at most 8 of
+      // its entries, the next 8 from the cursor.
       const uint32_t nv = sm.cnt_v;
-      uint32_t vcol = 0xFFFFFFFFu;
+      uint32_t vcol = 0xFFFFFFFFu, vk = 0, vend = 0;
       if (tid < nv) {
         const uint32_t idx = first + tid;
         uint32_t wd = 0;
@@ -1036,22 +1043,37 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
         vcol = wd * 32 + __ffs(m) - 1;
         const uint32_t v = lo * 32 + vcol;
         const uint64_t va = g.rp[v], vb = g.rp[v + 1];
-        const uint32_t vbs = rp_blk(va), vn = min(rp_blk(vb) - vbs, K);
-        for (uint32_t k = 0; k < vn; ++k) {
-          const uint64_t e = g.bent[vbs + k];
-          const uint32_t blk = (uint32_t)(e >> 32) - lo;
-          if (blk < K) sm.vbits[tid][blk] = (uint32_t)e;
-        }
+        vk = rp_blk(va);
+        vend = vk + min(rp_blk(vb) - vk, K);
       }
-      __syncthreads();
       for (uint32_t c = 0; c < KW; c += kTcChunk / 32) {
-        // Unpack this chunk: thread tid row tid of A (8 words = 16 groups of
-        // 16 bytes); B rows by all threads, a quarter row each.
-        for (uint32_t q = 0; q < kTcChunk / 32; ++q) {
-          uint4 x0, x1;
-          unpack32(sm.vbits[tid][c + q], x0, x1);
-          *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q)) = x0;
-          *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q + 1)) = x1;
+        // This chunk of row tid of A: the neighbour's entries in blocks
+        // [lo + c, lo + c + 8) (8 loads issued before any is used), unpacked
+        // to 8 words = 16 groups of 16 bytes. B rows by all threads, a
+        // quarter row each.
+        {
+          constexpr uint32_t kW = kTcChunk / 32;
+          uint64_t e[kW];
+#pragma unroll
+          for (uint32_t j = 0; j < kW; ++j) e[j] = vk + j < vend ? g.bent[vk + j] : ~0ull;
+          uint32_t wv[kW], used = 0;
+#pragma unroll
+          for (uint32_t q = 0; q < kW; ++q) wv[q] = 0u;
+#pragma unroll
+          for (uint32_t j = 0; j < kW; ++j) {
+            const uint32_t d = (uint32_t)(e[j] >> 32) - lo - c;  // a missing entry gives ~0 - lo - c >= 8
+            used += d < kW ? 1u : 0u;
+#pragma unroll
+            for (uint32_t q = 0; q < kW; ++q) wv[q] |= d == q ? (uint32_t)e[j] : 0u;
+          }
+          vk += used;
+#pragma unroll
+          for (uint32_t q = 0; q < kW; ++q) {
+            uint4 x0, x1;
+            unpack32(wv[q], x0, x1);
+            *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q)) = x0;
+            *reinterpret_cast<uint4*>(sm.a + tc_off(tid, 2 * q + 1)) = x1;
+          }
         }
         {
           const uint32_t r = tid & 31, q0 = (tid >> 5) * 2;
@@ -2512,9 +2534,8 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
         s.in_cnt, s.inl);
     TB_LAUNCH_CHECK();
     if (s.tile_engine == TRIBIT_TILES_TCGEN05)
-      k_tiles_tc<<<(unsigned)(sms * 2), kTcThreads, sizeof(TcSmem), st>>>(g, s.pieces, s.piece_off, stats, per_graph,
-                                                                           nullptr, cfg.tile_wait_polls,
-                                                                           cfg.tile_test_no_commit);
+      k_tiles_tc<<<(unsigned)(sms * kTcCtasPerSm), kTcThreads, sizeof(TcSmem), st>>>(
+          g, s.pieces, s.piece_off, stats, per_graph, nullptr, cfg.tile_wait_polls, cfg.tile_test_no_commit);
     else
       k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
           g, s.pieces, s.piece_off, stats, per_graph, nullptr);
@@ -2524,7 +2545,7 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
     TB_LAUNCH_CHECK();
     k_rows_global<<<(unsigned)sms, kCtaThreads, 0, st>>>(g, ovf_global, stats, per_graph);
     TB_LAUNCH_CHECK();
-    info.ctas = (uint64_t)(kHubCtasPerSm + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? 2 : 5) + 2) * sms;
+    info.ctas = (uint64_t)(kHubCtasPerSm + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? kTcCtasPerSm : 5) + 2) * sms;
     info.kernels = 4;
     return info;
   }
@@ -2535,9 +2556,8 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
       g, s.pieces, s.piece_off, stats, ovf_cta, per_graph, cfg.block_ns, s.heavy, s.piece_width);
   TB_LAUNCH_CHECK();
   if (s.tile_engine == TRIBIT_TILES_TCGEN05)
-    k_tiles_tc<<<(unsigned)(sms * 2), kTcThreads, sizeof(TcSmem), st>>>(g, s.pieces, s.piece_off, stats, per_graph,
-                                                                         cfg.block_ns, cfg.tile_wait_polls,
-                                                                         cfg.tile_test_no_commit);
+    k_tiles_tc<<<(unsigned)(sms * kTcCtasPerSm), kTcThreads, sizeof(TcSmem), st>>>(
+        g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns, cfg.tile_wait_polls, cfg.tile_test_no_commit);
   else
     k_tiles_mma<<<(unsigned)(sms * 5), kTileWarps * 32, kTileWarps * sizeof(TileSmem), st>>>(
         g, s.pieces, s.piece_off, stats, per_graph, cfg.block_ns);
@@ -2555,7 +2575,8 @@ LaunchInfo launch_count(const GraphView& graph, const Schedule& s, DeviceStats* 
                                                                      s.inl, s.inrow, stats, per_graph, cfg.block_ns);
   TB_LAUNCH_CHECK();
   if (cfg.variant_stop) TB_CUDA(cudaEventRecord(cfg.variant_stop, st));
-  info.ctas = 2ull * warp_grid + (2ull + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? 2ull : 5ull) + kHubCtasPerSm) * sms;
+  info.ctas = 2ull * warp_grid +
+              (2ull + (s.tile_engine == TRIBIT_TILES_TCGEN05 ? (uint64_t)kTcCtasPerSm : 5ull) + kHubCtasPerSm) * sms;
   info.kernels = 6;
   return info;
 }
