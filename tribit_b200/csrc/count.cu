@@ -862,15 +862,22 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_tiles_mma(GraphView g, cons
 // frees them before it exits, also after a failed wait.
 
 constexpr int kTcThreads = 128;
-constexpr uint32_t kTcChunk = 256;                 // K bytes (columns) unpacked per round
+// 128-column rounds (7 CTAs an SM) measured faster than 256 (4 CTAs): dense
+// cliques 0.276 vs 0.364 ms.
+#ifndef TB_TC_CHUNK
+#define TB_TC_CHUNK 128
+#endif
+constexpr uint32_t kTcChunk = TB_TC_CHUNK;         // K bytes (columns) unpacked per round
+constexpr uint32_t kTcWords = kTcChunk / 32;       // bit words of a row per round
+static_assert(kTcChunk == 128 || kTcChunk == 256, "a round is 4 or 8 MMAs of K = 32");
 constexpr uint32_t kTcDrainPolls = 1u << 22;       // bounded wait for committed MMAs after a failed wait
 
 
-// 49 KiB: four CTAs an SM (128 of the 512 TMEM columns), so one CTA's
-// operand gathering runs while another's MMAs do.
+// 29 KiB with 128-column rounds (49 KiB with 256): seven CTAs an SM (four),
+// so one CTA's operand gathering runs while another's MMAs do.
 struct TcSmem {
-  uint8_t a[kTileNbrPiece * kTcChunk];             // A: 128 rows x 256 K-bytes, core-matrix layout
-  uint8_t b[32 * kTcChunk];                        // B: 32 rows x 256 K-bytes
+  uint8_t a[kTileNbrPiece * kTcChunk];             // A: 128 rows x kTcChunk K-bytes, core-matrix layout
+  uint8_t b[32 * kTcChunk];                        // B: 32 rows x kTcChunk K-bytes
   uint32_t ubits[32][kTileMaxK];                   // the block's rows
   uint32_t vmask[kTileMaxK];                       // OR of the rows: V
   uint32_t vpre[kTileMaxK + 1];                    // popcount prefix of vmask
@@ -879,7 +886,7 @@ struct TcSmem {
   uint32_t tmem;
   uint32_t lo, K, amask, cnt_v, fail;
 };
-constexpr int kTcCtasPerSm = 4;
+constexpr int kTcCtasPerSm = kTcChunk == 256 ? 4 : 7;
 static_assert(kTileMaxK == 64, "the vmask prefix is one warp scan of two words a lane");
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -995,7 +1002,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
       if (first == 0 && w == 0)
         racc = tile_fallback(g, rb, reinterpret_cast<uint64_t*>(sm.a), reinterpret_cast<uint32_t*>(sm.b), per_graph);
     } else if (K > 0) {
-      const uint32_t KW = (K + 7) & ~7u;  // words, whole 256-column chunks
+      const uint32_t KW = (K + kTcWords - 1) & ~(kTcWords - 1);  // words, whole rounds
       for (uint32_t r = w; r < 32; r += kTcThreads / 32)
         for (uint32_t q = lane; q < KW; q += 32) sm.ubits[r][q] = 0u;
       __syncthreads();
@@ -1028,8 +1035,8 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
       __syncthreads();
       // Neighbour tid of the piece: the (first + tid)-th set bit of V. Its
       // bit row starts at or after block lo (v >= 32 lo) and ascends, so a
-      // cursor walks it chunk by chunk: a chunk's 8 words hold at most 8 of
-      // its entries, the next 8 from the cursor.
+      // cursor walks it chunk by chunk: a chunk's kTcWords words hold at most
+      // kTcWords of its entries, the next kTcWords from the cursor.
       const uint32_t nv = sm.cnt_v;
       uint32_t vcol = 0xFFFFFFFFu, vk = 0, vend = 0;
       if (tid < nv) {
@@ -1046,13 +1053,13 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
         vk = rp_blk(va);
         vend = vk + min(rp_blk(vb) - vk, K);
       }
-      for (uint32_t c = 0; c < KW; c += kTcChunk / 32) {
+      for (uint32_t c = 0; c < KW; c += kTcWords) {
         // This chunk of row tid of A: the neighbour's entries in blocks
-        // [lo + c, lo + c + 8) (8 loads issued before any is used), unpacked
-        // to 8 words = 16 groups of 16 bytes. B rows by all threads, a
-        // quarter row each.
+        // [lo + c, lo + c + kTcWords) (kTcWords loads issued before any is
+        // used), unpacked to kTcWords words = 2 kTcWords groups of 16 bytes.
+        // B rows by all threads, a quarter row each.
         {
-          constexpr uint32_t kW = kTcChunk / 32;
+          constexpr uint32_t kW = kTcWords;
           uint64_t e[kW];
 #pragma unroll
           for (uint32_t j = 0; j < kW; ++j) e[j] = vk + j < vend ? g.bent[vk + j] : ~0ull;
@@ -1076,8 +1083,8 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
           }
         }
         {
-          const uint32_t r = tid & 31, q0 = (tid >> 5) * 2;
-          for (uint32_t q = q0; q < q0 + 2; ++q) {
+          const uint32_t r = tid & 31, q0 = (tid >> 5) * (kTcWords / 4);
+          for (uint32_t q = q0; q < q0 + kTcWords / 4; ++q) {
             uint4 x0, x1;
             unpack32(sm.ubits[r][c + q], x0, x1);
             *reinterpret_cast<uint4*>(sm.b + tc_off(r, 2 * q)) = x0;
