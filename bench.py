@@ -10,7 +10,7 @@ HBM; preprocessing is timed separately, as the reference reports it. `e2e` is
 the same metric through the public C-ABI call tribit_count_edges on pinned
 host entries: H2D copy, preprocessing, counting and the D2H result inside,
 the mean wall time of --e2e-steps calls (5; each call's time in step_ms;
-Python's garbage collector run before each call and held off during it).
+Python's garbage collector run before the calls and held off during them).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload rmat24|rmat22|rmat20|chung_lu|planted]
@@ -115,18 +115,25 @@ def profiled_traffic(workload, dispatch):
     return None
 
 
-def wall_call(fn):
-    """(fn(), its wall time in s), Python's garbage collector run before the
-    call and held off during it: the library call allocates no Python objects,
-    so a collection inside it would time the interpreter's heap, not the call."""
-    gc.collect()
-    gc.disable()
-    try:
-        t0 = time.perf_counter()
-        out = fn()
-        return out, time.perf_counter() - t0
-    finally:
+class gc_held:
+    """Python's garbage collector run once before a timed loop and held off
+    during it: the library calls allocate almost no Python objects, so a
+    collection inside one would time the interpreter's heap, not the call."""
+
+    def __enter__(self):
+        gc.collect()
+        gc.disable()
+        return self
+
+    def __exit__(self, *exc):
         gc.enable()
+
+
+def wall_call(fn):
+    """(fn(), its wall time in s)."""
+    t0 = time.perf_counter()
+    out = fn()
+    return out, time.perf_counter() - t0
 
 
 class ClockSampler:
@@ -219,7 +226,8 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     if dispatch == "learned":
         c.load_model(model_path)
     counts, r = c.count_batch(host, off, nn)  # sizes the arena, prepares the batch
-    (counts, r), e2e_s = wall_call(lambda: c.count_batch(host, off, nn))
+    with gc_held():
+        (counts, r), e2e_s = wall_call(lambda: c.count_batch(host, off, nn))
     tune = c.autotune(reps=2)
     c.capture_count()
     s = torch.cuda.Stream(device=local)
@@ -256,13 +264,14 @@ def batch_measurement(tb, np, torch, local, dispatch, model_path, num_graphs=409
     c1.set_tuning(tune.ctas_per_sm, tune.piece_width, tune.tile_min_nnz, launch_model="auto")
     idx = np.linspace(0, num_graphs - 1, per_graph_sample).astype(int)
     k_ms, e2e_one = 0.0, 0.0
-    for g in idx:
-        lo, hi = int(off[g]), int(off[g + 1])
-        c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))  # sizes the arena
-        rg, dt = wall_call(lambda: c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g])))
-        e2e_one += dt
-        k_ms += rg.kernel_ms
-        assert rg.triangles == int(counts[g]), f"graph {g}: batch {counts[g]} vs single {rg.triangles}"
+    with gc_held():
+        for g in idx:
+            lo, hi = int(off[g]), int(off[g + 1])
+            c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g]))  # sizes the arena
+            rg, dt = wall_call(lambda: c1.count_edges_device(d[lo:].data_ptr(), hi - lo, int(nn[g])))
+            e2e_one += dt
+            k_ms += rg.kernel_ms
+            assert rg.triangles == int(counts[g]), f"graph {g}: batch {counts[g]} vs single {rg.triangles}"
     c1.close()
     scale = num_graphs / per_graph_sample
     batched_ms = ms
@@ -486,10 +495,11 @@ def main():
             c.load_model(model_path)
         c.count_edges(host, n)  # sizes the arena
         secs, last = [], None
-        for _ in range(args.e2e_steps):
-            torch.cuda.synchronize()
-            last, dt = wall_call(lambda: c.count_edges(host, n))
-            secs.append(dt)
+        with gc_held():
+            for _ in range(args.e2e_steps):
+                torch.cuda.synchronize()
+                last, dt = wall_call(lambda: c.count_edges(host, n))
+                secs.append(dt)
         c.close()
         assert last.triangles == res.triangles
         return reduce_replicas(dist, m, statistics.mean(secs), device)[1], last, secs
@@ -514,10 +524,11 @@ def main():
         c.set_stream_options(tier or "auto", 0)
         c.count_edges(src, n)
         secs, last = [], None
-        for _ in range(2):
-            torch.cuda.synchronize()
-            last, dt = wall_call(lambda: c.count_edges(src, n))
-            secs.append(dt)
+        with gc_held():
+            for _ in range(2):
+                torch.cuda.synchronize()
+                last, dt = wall_call(lambda: c.count_edges(src, n))
+                secs.append(dt)
         c.close()
         assert last.triangles == res.triangles
         t = reduce_replicas(dist, m, statistics.mean(secs), device)[1]
