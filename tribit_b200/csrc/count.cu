@@ -1068,7 +1068,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tiles_tc(GraphView g, const uint
           for (uint32_t q = 0; q < kW; ++q) wv[q] = 0u;
 #pragma unroll
           for (uint32_t j = 0; j < kW; ++j) {
-            const uint32_t d = (uint32_t)(e[j] >> 32) - lo - c;  // a missing entry gives ~0 - lo - c >= 8
+            const uint32_t d = (uint32_t)(e[j] >> 32) - lo - c;  // a missing entry: ~0 - lo - c >= kW
             used += d < kW ? 1u : 0u;
 #pragma unroll
             for (uint32_t q = 0; q < kW; ++q) wv[q] |= d == q ? (uint32_t)e[j] : 0u;
