@@ -1,5 +1,7 @@
 """Larger graphs: RMAT scales 20 and 24 against the oracle, and at scale 22
 the size-independent property that every orientation and dispatcher agrees."""
+import os
+
 import numpy as np
 import pytest
 
@@ -59,6 +61,28 @@ def test_degree_slot_rows_with_duplicates_and_loops():
         with tb.Counter(dispatch=mode) as c:
             r = c.count_edges(e, n)
             assert (r.triangles, r.edges) == want, mode
+
+
+@pytest.mark.parametrize("name,n,make", [
+    ("er", 1 << 20, lambda: tb.gen_er(1 << 20, 16 << 20, seed=41)),
+    ("chung_lu", 1 << 20, lambda: tb.gen_chung_lu(1 << 20, 16 << 20, 2.1, 3000.0, seed=42)),
+])
+def test_long_bitmap_piece_lists_match_oracle(name, n, make):
+    """Over a million bitmap pieces on one graph: sparse Erdos-Renyi rows, and
+    Chung-Lu rows from a few neighbours to thousands (split into pieces, the
+    longest staged as hashes), against the oracle, and the same count on
+    repeated launches of the prepared graph."""
+    e = make()
+    want = oracle.count(e, n)
+    for mode in ("bitmap", "learned"):
+        with tb.Counter(dispatch=mode) as c:
+            if mode == "learned":
+                c.load_model(os.path.join(os.path.dirname(tb.__file__), "models", "dispatch_mlp.bin"))
+            r = c.count_edges(e, n)
+            assert (r.triangles, r.edges) == want, (name, mode)
+            for _ in range(2):
+                c.launch_count()
+                assert c.read_count().triangles == want[0], (name, mode)
 
 
 def test_rmat22_modes_agree():
